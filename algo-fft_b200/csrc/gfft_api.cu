@@ -1,0 +1,313 @@
+// extern "C" entry points of libgfft.so (declared in include/gfft.h).
+//
+// Argument validation reproduces the reference's order and sentinel errors
+// so a Go wrapper behaves exactly like the CPU library on bad input:
+// plan.go:504-516 (batch), plan.go:574-584 (single), plan_strided.go:101-135
+// (strided).
+#include <climits>
+#include <cstring>
+#include <new>
+#include <string>
+#include "gfft_internal.h"
+
+namespace gfft {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+
+gfft_status cuda_status(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+  if (e == cudaErrorMemoryAllocation) return GFFT_ERR_OUT_OF_MEMORY;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GFFT_ERR_NO_DEVICE;
+  return GFFT_ERR_CUDA;
+}
+
+static cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+// Host-slice path: copy in, run, copy out, wait.  Staging memory comes from
+// the device's stream-ordered pool, so repeated calls do not hit cudaMalloc.
+static gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count) {
+  const size_t bytes = size_t(count) * size_t(p->core.n) * elem_bytes(p->core.prec);
+  cudaStream_t st = nullptr;
+  GFFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  void* d = nullptr;
+  cudaError_t e = cudaMallocAsync(&d, bytes, st);
+  gfft_status s = GFFT_OK;
+  if (e != cudaSuccess) {
+    s = cuda_status(e, "cudaMallocAsync");
+  } else {
+    e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) s = cuda_status(e, "cudaMemcpyAsync(H2D)");
+    if (s == GFFT_OK) s = core_exec(&p->core, dir, d, d, count, p->core.n, p->core.n, st);
+    if (s == GFFT_OK) {
+      e = cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) s = cuda_status(e, "cudaMemcpyAsync(D2H)");
+    }
+    cudaFreeAsync(d, st);
+  }
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess && s == GFFT_OK) s = cuda_status(e, "cudaStreamSynchronize");
+  cudaStreamDestroy(st);
+  return s;
+}
+
+}  // namespace gfft
+
+using namespace gfft;
+
+extern "C" {
+
+gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const gfft_plan_options* opts) {
+  clear_error();
+  if (!out) return GFFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (n < 1) {
+    set_error("n < 1");
+    return GFFT_ERR_INVALID_LENGTH;
+  }
+  if (precision != GFFT_COMPLEX64 && precision != GFFT_COMPLEX128) return GFFT_ERR_INVALID_ARGUMENT;
+  gfft_plan_options o{};
+  if (opts) o = *opts;
+  if (o.batch < 0 || o.stride < 0) return GFFT_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return GFFT_ERR_NO_DEVICE;
+  }
+  if (o.device < 0 || o.device >= ndev) return GFFT_ERR_INVALID_ARGUMENT;
+  GFFT_CUDA(cudaSetDevice(o.device));
+  auto* p = new (std::nothrow) gfft_plan;
+  if (!p) return GFFT_ERR_OUT_OF_MEMORY;
+  p->opts = o;
+  gfft_status s = core_init(&p->core, precision, n, o.device);
+  if (s != GFFT_OK) {
+    core_free(&p->core);
+    delete p;
+    return s;
+  }
+  *out = p;
+  return GFFT_OK;
+}
+
+void gfft_plan_close(gfft_plan* plan) {
+  if (!plan) return;
+  core_free(&plan->core);
+  delete plan;
+}
+
+int64_t gfft_plan_len(const gfft_plan* plan) { return plan ? plan->core.n : 0; }
+
+gfft_status gfft_plan_algorithm(const gfft_plan* plan, char* buf, size_t cap) {
+  if (!plan || !buf || cap == 0) return GFFT_ERR_INVALID_ARGUMENT;
+  std::strncpy(buf, plan->core.name.c_str(), cap - 1);
+  buf[cap - 1] = 0;
+  return GFFT_OK;
+}
+
+// plan.go:574-584 validateSlices.
+static gfft_status check_single(gfft_plan* p, const void* dst, int64_t dst_len, const void* src, int64_t src_len) {
+  if (!p) return GFFT_ERR_INVALID_ARGUMENT;
+  if (!dst || !src) return GFFT_ERR_NIL_SLICE;
+  if (dst_len != p->core.n || src_len != p->core.n) return GFFT_ERR_LENGTH_MISMATCH;
+  return GFFT_OK;
+}
+
+// plan.go:505-516.
+static gfft_status check_batch(gfft_plan* p, const void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                               int64_t count) {
+  if (!p) return GFFT_ERR_INVALID_ARGUMENT;
+  if (!dst || !src) return GFFT_ERR_NIL_SLICE;
+  if (count < 1) return GFFT_ERR_INVALID_LENGTH;
+  if (count > INT64_MAX / p->core.n) return GFFT_ERR_LENGTH_MISMATCH;
+  const int64_t required = count * p->core.n;
+  if (dst_len < required || src_len < required) return GFFT_ERR_LENGTH_MISMATCH;
+  return GFFT_OK;
+}
+
+static gfft_status do_single(gfft_plan* p, int dir, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                             void* stream) {
+  clear_error();
+  gfft_status s = check_single(p, dst, dst_len, src, src_len);
+  if (s != GFFT_OK) return s;
+  return core_exec(&p->core, dir, dst, src, 1, p->core.n, p->core.n, as_stream(stream));
+}
+
+static gfft_status do_batch(gfft_plan* p, int dir, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                            int64_t count, void* stream) {
+  clear_error();
+  gfft_status s = check_batch(p, dst, dst_len, src, src_len, count);
+  if (s != GFFT_OK) return s;
+  return core_exec(&p->core, dir, dst, src, count, p->core.n, p->core.n, as_stream(stream));
+}
+
+gfft_status gfft_forward(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len, void* stream) {
+  return do_single(p, -1, dst, dst_len, src, src_len, stream);
+}
+gfft_status gfft_inverse(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len, void* stream) {
+  return do_single(p, +1, dst, dst_len, src, src_len, stream);
+}
+gfft_status gfft_forward_batch(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                               int64_t count, void* stream) {
+  return do_batch(p, -1, dst, dst_len, src, src_len, count, stream);
+}
+gfft_status gfft_inverse_batch(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                               int64_t count, void* stream) {
+  return do_batch(p, +1, dst, dst_len, src, src_len, count, stream);
+}
+
+// plan_strided.go:101-135 validateStridedSlices.
+static gfft_status check_strided(gfft_plan* p, const void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                 int64_t stride) {
+  if (!p) return GFFT_ERR_INVALID_ARGUMENT;
+  if (!dst || !src) return GFFT_ERR_NIL_SLICE;
+  if (stride < 1) return GFFT_ERR_INVALID_STRIDE;
+  const int64_t n = p->core.n;
+  if (stride == 1) {
+    if (dst_len < n || src_len < n) return GFFT_ERR_LENGTH_MISMATCH;
+    return GFFT_OK;
+  }
+  const int64_t max_index = n - 1;
+  if (max_index > (INT64_MAX - 1) / stride) return GFFT_ERR_INVALID_STRIDE;
+  const int64_t required = 1 + max_index * stride;
+  if (dst_len < required || src_len < required) return GFFT_ERR_LENGTH_MISMATCH;
+  return GFFT_OK;
+}
+
+static gfft_status do_strided(gfft_plan* p, int dir, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                              int64_t stride, void* stream) {
+  clear_error();
+  gfft_status s = check_strided(p, dst, dst_len, src, src_len, stride);
+  if (s != GFFT_OK) return s;
+  const int64_t n = p->core.n;
+  if (stride == 1) return core_exec(&p->core, dir, dst, src, 1, n, n, as_stream(stream));
+  // Gather the column into a contiguous buffer, transform, scatter back
+  // (plan_strided.go:72-98): two strided 2-D copies around one transform.
+  cudaStream_t st = as_stream(stream);
+  const size_t es = elem_bytes(p->core.prec);
+  void* tmp = nullptr;
+  GFFT_CUDA(cudaMallocAsync(&tmp, size_t(n) * es, st));
+  cudaError_t e = cudaMemcpy2DAsync(tmp, es, src, size_t(stride) * es, es, size_t(n), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) {
+    s = core_exec(&p->core, dir, tmp, tmp, 1, n, n, st);
+    if (s == GFFT_OK) {
+      e = cudaMemcpy2DAsync(dst, size_t(stride) * es, tmp, es, es, size_t(n), cudaMemcpyDeviceToDevice, st);
+    }
+  }
+  cudaFreeAsync(tmp, st);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy2DAsync");
+  return s;
+}
+
+gfft_status gfft_forward_strided(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                 int64_t stride, void* stream) {
+  return do_strided(p, -1, dst, dst_len, src, src_len, stride, stream);
+}
+gfft_status gfft_inverse_strided(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                 int64_t stride, void* stream) {
+  return do_strided(p, +1, dst, dst_len, src, src_len, stride, stream);
+}
+
+gfft_status gfft_forward_host(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len) {
+  clear_error();
+  gfft_status s = check_single(p, dst, dst_len, src, src_len);
+  return s != GFFT_OK ? s : run_host(p, -1, dst, src, 1);
+}
+gfft_status gfft_inverse_host(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len) {
+  clear_error();
+  gfft_status s = check_single(p, dst, dst_len, src, src_len);
+  return s != GFFT_OK ? s : run_host(p, +1, dst, src, 1);
+}
+gfft_status gfft_forward_batch_host(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                    int64_t count) {
+  clear_error();
+  gfft_status s = check_batch(p, dst, dst_len, src, src_len, count);
+  return s != GFFT_OK ? s : run_host(p, -1, dst, src, count);
+}
+gfft_status gfft_inverse_batch_host(gfft_plan* p, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                    int64_t count) {
+  clear_error();
+  gfft_status s = check_batch(p, dst, dst_len, src, src_len, count);
+  return s != GFFT_OK ? s : run_host(p, +1, dst, src, count);
+}
+
+const char* gfft_status_string(int32_t status) {
+  switch (status) {
+    case GFFT_OK: return "ok";
+    case GFFT_ERR_INVALID_LENGTH: return "algo-fft: invalid FFT length";
+    case GFFT_ERR_NIL_SLICE: return "algo-fft: nil slice";
+    case GFFT_ERR_LENGTH_MISMATCH: return "algo-fft: slice length mismatch";
+    case GFFT_ERR_INVALID_STRIDE: return "algo-fft: invalid stride";
+    case GFFT_ERR_INVALID_SPECTRUM: return "algo-fft: invalid spectrum";
+    case GFFT_ERR_NOT_IMPLEMENTED: return "algo-fft: not implemented";
+    case GFFT_ERR_CUDA: return "gfft: CUDA error";
+    case GFFT_ERR_OUT_OF_MEMORY: return "gfft: out of memory";
+    case GFFT_ERR_TIMEOUT: return "gfft: device wait timed out";
+    case GFFT_ERR_NO_DEVICE: return "gfft: no CUDA device";
+    case GFFT_ERR_INVALID_ARGUMENT: return "gfft: invalid argument";
+    case GFFT_ERR_WISDOM: return "gfft: malformed wisdom";
+  }
+  return "gfft: unknown status";
+}
+
+const char* gfft_last_error(void) { return g_last_error.c_str(); }
+
+gfft_status gfft_device_count(int32_t* count) {
+  if (!count) return GFFT_ERR_INVALID_ARGUMENT;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+  *count = n;
+  return GFFT_OK;
+}
+
+gfft_status gfft_buffer_alloc(void** ptr, int64_t bytes) {
+  clear_error();
+  if (!ptr || bytes < 0) return GFFT_ERR_INVALID_ARGUMENT;
+  *ptr = nullptr;
+  GFFT_CUDA(cudaMalloc(ptr, size_t(bytes > 0 ? bytes : 1)));
+  return GFFT_OK;
+}
+
+gfft_status gfft_buffer_free(void* ptr) {
+  clear_error();
+  if (ptr) GFFT_CUDA(cudaFree(ptr));
+  return GFFT_OK;
+}
+
+gfft_status gfft_buffer_upload(void* dst_device, const void* src_host, int64_t bytes) {
+  clear_error();
+  if (!dst_device || !src_host || bytes < 0) return GFFT_ERR_INVALID_ARGUMENT;
+  GFFT_CUDA(cudaMemcpy(dst_device, src_host, size_t(bytes), cudaMemcpyHostToDevice));
+  return GFFT_OK;
+}
+
+gfft_status gfft_buffer_download(void* dst_host, const void* src_device, int64_t bytes) {
+  clear_error();
+  if (!dst_host || !src_device || bytes < 0) return GFFT_ERR_INVALID_ARGUMENT;
+  GFFT_CUDA(cudaMemcpy(dst_host, src_device, size_t(bytes), cudaMemcpyDeviceToHost));
+  return GFFT_OK;
+}
+
+gfft_status gfft_stream_create(void** stream) {
+  clear_error();
+  if (!stream) return GFFT_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = nullptr;
+  GFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  *stream = s;
+  return GFFT_OK;
+}
+
+gfft_status gfft_stream_synchronize(void* stream) {
+  clear_error();
+  GFFT_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  return GFFT_OK;
+}
+
+gfft_status gfft_stream_destroy(void* stream) {
+  clear_error();
+  if (stream) GFFT_CUDA(cudaStreamDestroy(as_stream(stream)));
+  return GFFT_OK;
+}
+
+}  // extern "C"

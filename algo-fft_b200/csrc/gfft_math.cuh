@@ -1,0 +1,172 @@
+// Complex arithmetic and in-register DFT codelets for the sm_100a kernels.
+//
+// Elements are interleaved (re, im) pairs: float2 for complex64 and double2
+// for complex128, the memory layout of Go's complex64/complex128 slices.
+// Direction DIR is -1 for the forward transform exp(-2πi jk/n) and +1 for
+// the inverse, as in the reference (plan.go:320-330, 372-385).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "gfft_constants.cuh"
+
+namespace gfft {
+
+template <typename R> struct CxOf;
+template <> struct CxOf<float> { using type = float2; };
+template <> struct CxOf<double> { using type = double2; };
+template <typename R> using Cx = typename CxOf<R>::type;
+
+template <typename C> struct RealOf;
+template <> struct RealOf<float2> { using type = float; };
+template <> struct RealOf<double2> { using type = double; };
+
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { return C{a.x + b.x, a.y + b.y}; }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { return C{a.x - b.x, a.y - b.y}; }
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+  return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return C{a.x, -a.y}; }
+template <typename C, typename R> __host__ __device__ __forceinline__ C cscale(C a, R s) { return C{a.x * s, a.y * s}; }
+
+// a * (DIR * i): forward multiplies by -i, inverse by +i.
+template <int DIR, typename C> __device__ __forceinline__ C mul_di(C a) {
+  if constexpr (DIR > 0) return C{-a.y, a.x};
+  else return C{a.y, -a.x};
+}
+
+// a * exp(DIR * 2πi * M / R) for a compile-time root; the quarter-turn
+// cases are exact sign swaps.
+template <int R, int M, int DIR, typename C> __device__ __forceinline__ C twc(C a) {
+  using Re = typename RealOf<C>::type;
+  constexpr int m = ((M % R) + R) % R;
+  if constexpr (m == 0) return a;
+  else if constexpr (2 * m == R) return C{-a.x, -a.y};
+  else if constexpr (4 * m == R) return mul_di<DIR>(a);
+  else if constexpr (4 * m == 3 * R) return mul_di<-DIR>(a);
+  else {
+    static_assert(64 % R == 0, "constant roots cover R | 64");
+    constexpr double c = kCos64[m * (64 / R)];
+    constexpr double s = DIR * kSin64[m * (64 / R)];
+    return C{Re(c) * a.x - Re(s) * a.y, Re(c) * a.y + Re(s) * a.x};
+  }
+}
+
+template <int R> constexpr double cos_r(int m) {
+  return R == 3 ? kCos3[m] : R == 5 ? kCos5[m] : kCos7[m];
+}
+template <int R> constexpr double sin_r(int m) {
+  return R == 3 ? kSin3[m] : R == 5 ? kSin5[m] : kSin7[m];
+}
+
+// Odd prime radix (3, 5, 7): pairs s_j = v_j + v_{R-j}, d_j = v_j - v_{R-j};
+// X_k = v0 + Σ cos(2πjk/R) s_j  ±  DIR·i Σ sin(2πjk/R) d_j.
+template <int R, int DIR, typename C> __device__ __forceinline__ void dft_odd(C* v) {
+  using Re = typename RealOf<C>::type;
+  constexpr int H = (R - 1) / 2;
+  C s[H + 1], d[H + 1];
+#pragma unroll
+  for (int j = 1; j <= H; ++j) {
+    s[j] = cadd(v[j], v[R - j]);
+    d[j] = csub(v[j], v[R - j]);
+  }
+  C x0 = v[0];
+  C sum = x0;
+#pragma unroll
+  for (int j = 1; j <= H; ++j) sum = cadd(sum, s[j]);
+#pragma unroll
+  for (int k = 1; k <= H; ++k) {
+    C a = x0, b = C{0, 0};
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+      const Re c = Re(cos_r<R>((j * k) % R));
+      const Re sn = Re(sin_r<R>((j * k) % R));
+      a.x += c * s[j].x;
+      a.y += c * s[j].y;
+      b.x += sn * d[j].x;
+      b.y += sn * d[j].y;
+    }
+    C ib = mul_di<DIR>(b);
+    v[k] = cadd(a, ib);
+    v[R - k] = csub(a, ib);
+  }
+  v[0] = sum;
+}
+
+template <int R, int R1, int R2, int DIR, int IDX = 0, typename C>
+__device__ __forceinline__ void twiddle_block(C* a) {
+  if constexpr (IDX < R) {
+    constexpr int n2 = IDX / R1, k1 = IDX % R1;
+    a[IDX] = twc<R, n2 * k1, DIR>(a[IDX]);
+    twiddle_block<R, R1, R2, DIR, IDX + 1>(a);
+  }
+}
+
+// In-register DFT of R points, natural order in and out.  Powers of two are
+// split R = R1 * R2 (n = R2 n1 + n2, k = k1 + R1 k2): R2 DFTs of size R1,
+// constant twiddles W_R^{n2 k1}, R1 DFTs of size R2.
+template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) {
+  if constexpr (R == 1) {
+  } else if constexpr (R == 2) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = mul_di<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  } else if constexpr (R == 3 || R == 5 || R == 7) {
+    dft_odd<R, DIR>(v);
+  } else {
+    static_assert(R == 8 || R == 16 || R == 32 || R == 64, "unsupported radix");
+    constexpr int R1 = (R == 8) ? 2 : 4;
+    constexpr int R2 = R / R1;
+    C a[R];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) {
+      C t[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
+      dft<R1, DIR>(t);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) a[n2 * R1 + k1] = t[k1];
+    }
+    // constant twiddles, unrolled through a helper so M is compile-time
+    twiddle_block<R, R1, R2, DIR>(a);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      C t[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) t[n2] = a[n2 * R1 + k1];
+      dft<R2, DIR>(t);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+  }
+}
+
+// v[r] *= w^r (r = 1..RS-1) where w = tw[m] (conjugated for the inverse).
+// Powers are built as w^r = w^{floor(r/2)} * w^{ceil(r/2)}, a product tree
+// of depth ceil(log2 r), so each power carries a few ulp at most.
+template <int RS, int DIR, typename C>
+__device__ __forceinline__ void apply_twiddles(C* v, C w1) {
+  if constexpr (RS > 1) {
+    if constexpr (DIR > 0) w1.y = -w1.y;
+    C w[RS];
+    w[1] = w1;
+#pragma unroll
+    for (int r = 2; r < RS; ++r) w[r] = cmul(w[r / 2], w[r - r / 2]);
+#pragma unroll
+    for (int r = 1; r < RS; ++r) v[r] = cmul(v[r], w[r]);
+  }
+}
+
+// Streaming global accesses: the batch is touched exactly once.
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(float2* p, float2 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_stream(double2* p, double2 v) { __stcs(p, v); }
+
+}  // namespace gfft

@@ -1,0 +1,122 @@
+// Single-pass shared-memory Stockham kernel for power-of-two N (K1).
+//
+// One transform is owned by T = N/EPT threads; each thread holds EPT
+// elements in registers.  Stage s (radix RS, p = product of the previous
+// radices) is Stockham's self-sorting step: butterfly i reads
+// x[i + r*N/RS], multiplies by W_{p*RS}^{r*k} (k = i mod p), runs DFT_RS in
+// registers and writes y[(i-k)*RS + k + r*p].  The first stage reads
+// straight from HBM and the last writes straight to HBM, both at unit
+// stride across the T threads (fully coalesced), so shared memory carries
+// only the exchanges in between.  Shared memory is padded by one element
+// every EPT elements, which makes every exchange pattern bank-conflict free
+// for EPT >= 8 (checked exhaustively on the CPU for each schedule).
+//
+// Replaces the reference's size-specific DIT codelets 4..16384
+// (internal/kernels/codelet_init.go:60-440) and the radix-2 Stockham
+// (internal/kernels/stockham.go:21) for one batch of transforms
+// (plan.go:504-571).
+#pragma once
+#include "gfft_math.cuh"
+
+namespace gfft {
+
+template <int N, int EPT, int ES>
+struct Pow2Shape {
+  static constexpr int T = N / EPT;                        // threads per transform
+  static constexpr int TPB = T >= 256 ? T : 256;           // threads per CTA
+  static constexpr int B = TPB / T;                        // transforms per CTA
+  static constexpr int PSH = EPT == 2 ? 1 : EPT == 4 ? 2 : EPT == 8 ? 3 : EPT == 16 ? 4 : 5;
+  static constexpr int PAD_EXTRA = (T < 16) ? 1 : 0;
+  static constexpr int STRIDE = (N - 1) + ((N - 1) >> PSH) + 1 + PAD_EXTRA;  // per transform
+  static constexpr int SMEM = (N == EPT) ? 0 : B * STRIDE * ES;               // bytes per CTA
+  __host__ __device__ static constexpr int pad(int e) { return e + (e >> PSH); }
+};
+
+template <int T>
+__device__ __forceinline__ void xsync() {
+  if constexpr (T <= 32) __syncwarp();
+  else __syncthreads();
+}
+
+template <typename C, int N, int EPT, int DIR, int P>
+__device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int t, bool valid,
+                                           const C* __restrict__ tw,
+                                           typename RealOf<C>::type scale) {
+  using S = Pow2Shape<N, EPT, sizeof(C)>;
+  constexpr int T = S::T;
+  constexpr int RS = (P * EPT <= N) ? EPT : N / P;
+  constexpr int Q = EPT / RS;
+  constexpr int STRIDE = N / RS;
+  constexpr bool FIRST = (P == 1);
+  constexpr bool LAST = (P * RS == N);
+
+  if constexpr (FIRST) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+      for (int r = 0; r < RS; ++r) {
+        const int e = t + q * T + r * STRIDE;
+        v[q * RS + r] = valid ? ld_stream(in + e) : C{0, 0};
+      }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+      for (int r = 0; r < RS; ++r) v[q * RS + r] = sh[S::pad(t + q * T + r * STRIDE)];
+  }
+
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if constexpr (P > 1) {
+      const int i = t + q * T;
+      const int k = i & (P - 1);
+      apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + k * (N / (P * RS))));
+    }
+    dft<RS, DIR>(v + q * RS);
+  }
+
+  if constexpr (LAST) {
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) {
+          const int e = t + q * T + r * P;
+          st_stream(out + e, cscale(v[q * RS + r], scale));
+        }
+    }
+  } else {
+    if constexpr (!FIRST) xsync<T>();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int i = t + q * T;
+      const int k = i & (P - 1);
+      const int j = (i - k) * RS + k;
+#pragma unroll
+      for (int r = 0; r < RS; ++r) sh[S::pad(j + r * P)] = v[q * RS + r];
+    }
+    xsync<T>();
+    pow2_stage<C, N, EPT, DIR, P * RS>(v, in, out, sh, t, valid, tw, scale);
+  }
+}
+
+// Batched C2C: transform b reads src[b*idist .. b*idist+N) and writes
+// dst[b*odist ..).  src may equal dst (every CTA reads its whole transform
+// before it writes any of it).  tw holds W_N^m, m < N, in the element type.
+template <typename C, int N, int EPT, int DIR>
+__global__ void __launch_bounds__(Pow2Shape<N, EPT, sizeof(C)>::TPB)
+k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const C* __restrict__ tw,
+       typename RealOf<C>::type scale) {
+  using S = Pow2Shape<N, EPT, sizeof(C)>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw) + (threadIdx.x / S::T) * S::STRIDE;
+  const int t = threadIdx.x % S::T;
+  const int64_t b = int64_t(blockIdx.x) * S::B + threadIdx.x / S::T;
+  const bool valid = b < count;
+  const C* in = src + (valid ? b * idist : 0);
+  C* out = dst + (valid ? b * odist : 0);
+  C v[EPT];
+  pow2_stage<C, N, EPT, DIR, 1>(v, in, out, sh, t, valid, tw, scale);
+}
+
+}  // namespace gfft

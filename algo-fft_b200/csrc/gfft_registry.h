@@ -1,0 +1,31 @@
+// Kernel registry: every compiled kernel variant with its launch shape, so
+// plans and the autotuner can pick among them at run time.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+namespace gfft {
+
+enum Prec { kC64 = 0, kC128 = 1 };
+
+// Single-pass power-of-two kernel (k_pow2) of one (precision, N, EPT, dir).
+struct Pow2Kernel {
+  int prec, n, ept, dir;
+  int tpb;        // threads per CTA
+  int per_cta;    // transforms per CTA
+  int smem;       // dynamic shared memory bytes per CTA
+  const void* func;
+  cudaError_t (*launch)(const void* src, void* dst, int64_t count, int64_t idist, int64_t odist,
+                        const void* tw, double scale, cudaStream_t st);
+};
+
+void register_pow2(const Pow2Kernel& k);
+const Pow2Kernel* find_pow2(int prec, int n, int ept, int dir);
+std::vector<const Pow2Kernel*> pow2_variants(int prec, int n, int dir);
+
+// Ensures every registered kernel has its shared-memory limit raised (once
+// per device).
+cudaError_t prepare_kernels();
+
+}  // namespace gfft

@@ -1,0 +1,308 @@
+"""Benchmark of the batched complex64 C2C path (Plan.ForwardBatch) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): one ForwardBatch per length of the power-of-two sweep,
+each over a 1 GiB batch of complex64 (count = 2^27 / N transforms), inputs
+i.i.d. N(0,1) from a fixed seed, resident in HBM.  Every batch is larger than
+the 126 MB L2, so no flush is needed between steps.  The metric is
+algorithmic HBM bandwidth: 16*N bytes per transform (one read and one write
+of 8*N bytes) divided by device time.
+
+Multi-GPU (torchrun): batches shard across ranks (each rank runs the same
+per-rank workload, no collective on the data path, weak scaling); time is the
+max over ranks.
+
+--impl reference times the reference's CPU algorithms (the oracle's C++
+restatement of the pure-Go path; no Go toolchain exists on the box) on all
+host threads over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "algo-fft_b200"))
+
+BUF_BYTES = 1 << 30                      # one 1 GiB batch per length
+SWEEP = [2 ** k for k in range(10, 15)]  # lengths with a single-pass schedule
+WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^10..2^14, 1 GiB batch per N"
+
+
+def bytes_per_transform(n: int) -> int:
+    return 16 * n
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while timing."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._p = None
+
+    def __enter__(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(sample_seconds: float = 12.0):
+    """The oracle's restatement of the reference CPU path, all host threads,
+    on a bounded sample of each length of the sweep."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    threads = os.cpu_count() or 1
+    per_n = sample_seconds / len(SWEEP)
+    total_bytes, total_t, sample = 0, 0.0, []
+    rng = np.random.default_rng(0)
+    for n in SWEEP:
+        count = max(threads, (1 << 22) // n)
+        x = (rng.standard_normal(n * count) + 1j * rng.standard_normal(n * count)).astype(np.complex64)
+        t0 = time.perf_counter()
+        oracle.batch(x, n, nthreads=threads)
+        dt = time.perf_counter() - t0
+        reps = max(1, int(per_n / max(dt, 1e-6)))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            oracle.batch(x, n, nthreads=threads)
+        dt = time.perf_counter() - t0
+        total_bytes += reps * count * bytes_per_transform(n)
+        total_t += dt
+        sample.append(f"N={n}x{count}x{reps}")
+    return {"value": total_bytes / total_t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": "oracle C++ restatement of the reference pure-Go path, " + ", ".join(sample)}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(sample_seconds=2.0)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(sample_seconds=6.0))
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": "FFT HBM GB/s (% of peak) at stated err", "value": v, "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32)", "data": "synthetic N(0,1), seed 0",
+            "config": {"workload": WORKLOAD, "sizes": SWEEP}, "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import algofft
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    plans, bufs = {}, {}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    for n in SWEEP:
+        count = BUF_BYTES // (8 * n)
+        plans[n] = algofft.NewPlan(n)
+        x = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+        bufs[n] = (x, torch.empty_like(x), count)
+
+    def step(evs=None):
+        for i, n in enumerate(SWEEP):
+            x, y, count = bufs[n]
+            plans[n].ForwardBatch(y, x, count)
+            if evs is not None:
+                evs[i].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+
+    per_size_ms = {n: 0.0 for n in SWEEP}
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for s in range(args.steps):
+            evs = [torch.cuda.Event(enable_timing=True) for _ in SWEEP]
+            t0 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            step(evs)
+            torch.cuda.synchronize()
+            prev = t0
+            for i, n in enumerate(SWEEP):
+                per_size_ms[n] += prev.elapsed_time(evs[i])
+                prev = evs[i]
+        end.record(stream)
+        torch.cuda.synchronize()
+    total_ms = start.elapsed_time(end)
+    dev_ms = sum(per_size_ms.values())  # kernels only (host gaps between steps excluded)
+    t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    dev_ms = float(t.item())
+    bytes_step = sum(bytes_per_transform(n) * bufs[n][2] for n in SWEEP)
+    value = world * bytes_step * args.steps / (dev_ms / 1e3) / 1e9
+
+    # dominant kernel: the length with the largest share of device time
+    dom = max(SWEEP, key=lambda n: per_size_ms[n])
+    dom_ms = per_size_ms[dom] / args.steps
+    dom_bytes = bytes_per_transform(dom) * bufs[dom][2]
+    peak, peak_kind = peak_hbm()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+
+    # correctness at the stated error on the first transforms of each batch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    errs = {}
+    for n in SWEEP:
+        x, y, count = bufs[n]
+        xs = x[: n * 2].cpu().numpy().astype(np.complex128)
+        ys = y[: n * 2].cpu().numpy().astype(np.complex128)
+        ref = oracle.batch(xs, n)
+        errs[n] = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
+
+    # end to end: the same sweep through the host-slice API (pinned host
+    # buffers, H2D + transform + D2H inside the timed region, every step)
+    e2e_steps = max(1, min(args.steps, 3))
+    host = {}
+    for n in SWEEP:
+        x, y, count = bufs[n]
+        hx = torch.empty(x.numel(), dtype=torch.complex64, pin_memory=True)
+        hx.copy_(x)
+        hy = torch.empty_like(hx, pin_memory=True)
+        host[n] = (hx.numpy(), hy.numpy(), count)
+    for n in SWEEP:  # warm the staging pool
+        hx, hy, count = host[n]
+        plans[n].ForwardBatch(hy, hx, count)
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for n in SWEEP:
+            hx, hy, count = host[n]
+            plans[n].ForwardBatch(hy, hx, count)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if pg:
+        pg.all_reduce(te, op=pg.ReduceOp.MAX)
+    e2e_val = world * bytes_step * e2e_steps / float(te.item()) / 1e9
+
+    if rank == 0:
+        line = {
+            "metric": "FFT HBM GB/s (% of peak) at stated err", "value": value, "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 (f32 arithmetic)",
+            "data": "synthetic N(0,1) seeded, resident in HBM",
+            "config": {"workload": WORKLOAD, "sizes": SWEEP, "batch_bytes": BUF_BYTES,
+                       "l2": "inputs (1 GiB per batch) larger than the 126 MB L2; no flush",
+                       "parallelism": f"batch sharding x{world} (no collective)"},
+            "per_size_gbs": {str(n): bytes_per_transform(n) * bufs[n][2] * args.steps / (per_size_ms[n] / 1e3) / 1e9
+                             for n in SWEEP},
+            "rel_l2_vs_fp64": {str(n): errs[n] for n in SWEEP},
+            "roofline": {"bound": "hbm", "kernel": f"k_pow2 N={dom} ({plans[dom].Algorithm()})",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": dom_bytes},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": bytes_step // 2,
+                    "d2h_bytes_per_step": bytes_step // 2, "steps": e2e_steps,
+                    "path": "Plan.ForwardBatch on pinned host slices (gfft_forward_batch_host)"},
+            "gpu_launches": args.steps * len(SWEEP),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    for p in plans.values():
+        p.Close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

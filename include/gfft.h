@@ -1,0 +1,162 @@
+/*
+ * gfft.h — C ABI of the B200 (sm_100a) FFT engine behind algo-fft's
+ * batched-transform path.
+ *
+ * Every entry point takes plain pointers and sizes and returns a status code,
+ * so a cgo binding can call it directly.  Each entry
+ * point names the reference API it replaces as file:line inside
+ * CWBudde/algo-fft.
+ *
+ * Conventions
+ *  - Complex data is interleaved (re, im): complex64 = 2 x float32,
+ *    complex128 = 2 x float64, exactly Go's []complex64 / []complex128 layout.
+ *  - Lengths (`*_len`) are counted in elements of the slice type, as Go's
+ *    len() would report them.
+ *  - Functions without the `_host` suffix take DEVICE pointers (the
+ *    gpu.Buffer path, gpu/backend.go:29-37) and are ordered on `stream`
+ *    (a cudaStream_t; NULL = the legacy default stream).  They return as soon
+ *    as the work is queued.
+ *  - Functions with the `_host` suffix take HOST pointers (the Go-slice
+ *    path): they copy in, compute and copy out before returning, and retain
+ *    no pointer after they return (cgo pointer rules).
+ *  - Forward transforms are unscaled; inverse transforms scale by 1/n
+ *    (plan.go:320-330, 372-385).
+ *  - A plan is immutable after creation and may be used from several threads
+ *    at once (plan.go:13-17); host-call staging buffers are per call.
+ */
+#ifndef GFFT_H
+#define GFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GFFT_API __attribute__((visibility("default")))
+#else
+#define GFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..6 map one-to-one onto the reference's sentinel errors
+ * (errors.go:6-30); the Go binding converts them back to those values so
+ * errors.Is keeps working.  100+ are device-side conditions the CPU library
+ * never had. */
+typedef enum gfft_status {
+  GFFT_OK = 0,
+  GFFT_ERR_INVALID_LENGTH = 1,   /* ErrInvalidLength   errors.go:11 */
+  GFFT_ERR_NIL_SLICE = 2,        /* ErrNilSlice        errors.go:14 */
+  GFFT_ERR_LENGTH_MISMATCH = 3,  /* ErrLengthMismatch  errors.go:18 */
+  GFFT_ERR_INVALID_STRIDE = 4,   /* ErrInvalidStride   errors.go:22 */
+  GFFT_ERR_INVALID_SPECTRUM = 5, /* ErrInvalidSpectrum errors.go:26 */
+  GFFT_ERR_NOT_IMPLEMENTED = 6,  /* ErrNotImplemented  errors.go:30 */
+  GFFT_ERR_CUDA = 100,           /* a CUDA runtime call failed */
+  GFFT_ERR_OUT_OF_MEMORY = 101,  /* device or pinned-host allocation failed */
+  GFFT_ERR_TIMEOUT = 102,        /* a bounded device wait gave up */
+  GFFT_ERR_NO_DEVICE = 103,      /* no CUDA device (gpu.ErrBackendUnavailable) */
+  GFFT_ERR_INVALID_ARGUMENT = 104,
+  GFFT_ERR_WISDOM = 105          /* malformed wisdom text */
+} gfft_status;
+
+/* gpu/types.go:11-14 PrecisionKind. */
+typedef enum gfft_precision { GFFT_COMPLEX64 = 0, GFFT_COMPLEX128 = 1 } gfft_precision;
+
+/* plan_options.go:15-33 PlannerMode. */
+enum { GFFT_PLANNER_ESTIMATE = 0, GFFT_PLANNER_MEASURE = 1, GFFT_PLANNER_PATIENT = 2, GFFT_PLANNER_EXHAUSTIVE = 3 };
+
+/* internal/fftypes/strategy.go:4-13 KernelStrategy. */
+enum {
+  GFFT_KERNEL_AUTO = 0, GFFT_KERNEL_DIT = 1, GFFT_KERNEL_STOCKHAM = 2, GFFT_KERNEL_SIXSTEP = 3,
+  GFFT_KERNEL_EIGHTSTEP = 4, GFFT_KERNEL_BLUESTEIN = 5, GFFT_KERNEL_RECURSIVE = 6
+};
+
+/* plan_options.go:46-76 PlanOptions (Radices and Workspace are accepted by
+ * the reference but unused; Wisdom is the process-wide store below) plus
+ * gpu/types.go:32-42 DeviceIndex. */
+typedef struct gfft_plan_options {
+  int32_t planner;  /* GFFT_PLANNER_* */
+  int32_t strategy; /* GFFT_KERNEL_* */
+  int64_t batch;    /* PlanOptions.Batch (0 = 1) */
+  int64_t stride;   /* PlanOptions.Stride (0 = contiguous) */
+  int32_t in_place; /* PlanOptions.InPlace */
+  int32_t device;   /* gpu.PlanOptions.DeviceIndex */
+} gfft_plan_options;
+
+/* Opaque 1-D complex plan: Plan[T] (plan.go:18). */
+typedef struct gfft_plan gfft_plan;
+
+/* ---- plan lifecycle ---------------------------------------------------- */
+
+/* NewPlanT[T](n) / NewPlanWithOptions (plan.go:596-603; NewPlan32/NewPlan64
+ * plan.go:1013-1027).  opts may be NULL.  n < 1 -> GFFT_ERR_INVALID_LENGTH. */
+GFFT_API gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const gfft_plan_options* opts);
+
+/* Plan.Close (plan.go:1223).  NULL is ignored. */
+GFFT_API void gfft_plan_close(gfft_plan* plan);
+
+/* Plan.Len (plan.go:148). */
+GFFT_API int64_t gfft_plan_len(const gfft_plan* plan);
+
+/* Plan.Algorithm (plan.go:159): the bound GPU schedule as a
+ * NUL-terminated string, e.g. "gpu:sm100:pow2:n1024:ept32". */
+GFFT_API gfft_status gfft_plan_algorithm(const gfft_plan* plan, char* buf, size_t cap);
+
+/* ---- device-resident execution (gpu.PlanImpl, gpu/backend.go:44-51) ---- */
+
+/* Plan.Forward / Inverse (plan.go:332,382): one transform; dst may equal src. */
+GFFT_API gfft_status gfft_forward(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len, void* stream);
+GFFT_API gfft_status gfft_inverse(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len, void* stream);
+
+/* Plan.ForwardBatch / InverseBatch (plan.go:504-571): count transforms on
+ * [i*n, (i+1)*n).  Validation order: nil -> count < 1 -> lengths. */
+GFFT_API gfft_status gfft_forward_batch(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                               int64_t count, void* stream);
+GFFT_API gfft_status gfft_inverse_batch(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                               int64_t count, void* stream);
+
+/* Plan.ForwardStrided / InverseStrided (plan_strided.go:16,25): one
+ * transform over src[i*stride], written to dst[i*stride]. */
+GFFT_API gfft_status gfft_forward_strided(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                 int64_t stride, void* stream);
+GFFT_API gfft_status gfft_inverse_strided(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                 int64_t stride, void* stream);
+
+/* ---- host-slice execution (the Go-slice methods) ------------------------ */
+
+GFFT_API gfft_status gfft_forward_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len);
+GFFT_API gfft_status gfft_inverse_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len);
+GFFT_API gfft_status gfft_forward_batch_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                    int64_t count);
+GFFT_API gfft_status gfft_inverse_batch_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                    int64_t count);
+
+/* ---- errors -------------------------------------------------------------- */
+
+/* Text of a status code (the reference's error strings for 1..6). */
+GFFT_API const char* gfft_status_string(int32_t status);
+/* Detail of the last failure on the calling thread ("" if none). */
+GFFT_API const char* gfft_last_error(void);
+
+/* ---- devices, streams and buffers (gpu.Context / Buffer / Stream) ------- */
+
+/* Backend.Devices (gpu/backend.go:10): number of CUDA devices (0 if none). */
+GFFT_API gfft_status gfft_device_count(int32_t* count);
+/* Context.NewBuffer (gpu/backend.go:18): device allocation of `bytes`. */
+GFFT_API gfft_status gfft_buffer_alloc(void** ptr, int64_t bytes);
+/* Buffer.Close (gpu/backend.go:36). */
+GFFT_API gfft_status gfft_buffer_free(void* ptr);
+/* Buffer.Upload / Download (gpu/backend.go:32-35): synchronous copies. */
+GFFT_API gfft_status gfft_buffer_upload(void* dst_device, const void* src_host, int64_t bytes);
+GFFT_API gfft_status gfft_buffer_download(void* dst_host, const void* src_device, int64_t bytes);
+/* Context.NewStream / Stream.Synchronize / Stream.Close (gpu/backend.go:19,40-41). */
+GFFT_API gfft_status gfft_stream_create(void** stream);
+GFFT_API gfft_status gfft_stream_synchronize(void* stream);
+GFFT_API gfft_status gfft_stream_destroy(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GFFT_H */
