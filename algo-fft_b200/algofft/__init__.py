@@ -11,6 +11,9 @@ from .plan import (COMPLEX64, COMPLEX128, KernelAuto, KernelBluestein, KernelDIT
                    KernelSixStep, KernelStockham, NewPlan, NewPlan32, NewPlan64, NewPlanT, NewPlanWithOptions, Plan,
                    PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerMeasure, PlannerPatient)
 
+from .wisdom import (Autotune, ClearWisdom, ExportWisdom, ExportWisdomToString, ImportWisdom,
+                     ImportWisdomFromString, Variants, WisdomLen)
+
 lib()  # fail loudly at import when the native library is absent
 
 

@@ -90,6 +90,16 @@ SIGNATURES = {
     "gfft_plan_close": (None, [P]),
     "gfft_plan_len": (I64, [P]),
     "gfft_plan_algorithm": (I32, [P, CHARP, SZ]),
+    "gfft_plan_new_variant": (I32, [PP, I32, I64, CHARP]),
+    "gfft_plan_variants": (I32, [I32, I64, CHARP, SZ, ctypes.POINTER(SZ)]),
+    "gfft_plan_check": (I32, [P]),
+    "gfft_autotune": (I32, [I32, I64, I64, I32, CHARP, SZ, ctypes.POINTER(SZ)]),
+    "gfft_wisdom_import_string": (I32, [CHARP]),
+    "gfft_wisdom_export_string": (I32, [CHARP, SZ, ctypes.POINTER(SZ)]),
+    "gfft_wisdom_import_file": (I32, [CHARP]),
+    "gfft_wisdom_export_file": (I32, [CHARP]),
+    "gfft_wisdom_clear": (None, []),
+    "gfft_wisdom_len": (I64, []),
     "gfft_forward": (I32, [P, P, I64, P, I64, P]),
     "gfft_inverse": (I32, [P, P, I64, P, I64, P]),
     "gfft_forward_batch": (I32, [P, P, I64, P, I64, I64, P]),

@@ -68,12 +68,20 @@ def _dtype_prec(dtype) -> int:
 class Plan:
     """Plan[T] (plan.go:18).  T is complex64 (precision 0) or complex128."""
 
-    def __init__(self, n: int, precision: int = COMPLEX64, opts: PlanOptions | None = None):
+    def __init__(self, n: int, precision: int = COMPLEX64, opts: PlanOptions | None = None,
+                 variant: str | None = None):
         self._h = ctypes.c_void_p()
         self.precision = precision
         self._opts = opts or PlanOptions()
-        c_opts = self._opts.to_c()
-        check(lib().gfft_plan_new(ctypes.byref(self._h), precision, n, ctypes.byref(c_opts)))
+        if variant is not None:
+            check(lib().gfft_plan_new_variant(ctypes.byref(self._h), precision, n, variant.encode()))
+        else:
+            c_opts = self._opts.to_c()
+            check(lib().gfft_plan_new(ctypes.byref(self._h), precision, n, ctypes.byref(c_opts)))
+
+    def Check(self) -> None:
+        """Raises ErrTimeout if a bounded device wait of this plan expired."""
+        check(lib().gfft_plan_check(self._h))
 
     # -- lifecycle ---------------------------------------------------------
     def Close(self) -> None:

@@ -5,6 +5,7 @@
 // plan.go:504-516 (batch), plan.go:574-584 (single), plan_strided.go:101-135
 // (strided).
 #include <climits>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
@@ -81,7 +82,21 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts = o;
-  gfft_status s = core_init(&p->core, precision, n, o.device);
+  // PlannerMeasure/Patient/Exhaustive (plan_options.go:15-33): time the
+  // compiled variants once and remember the winner in the wisdom store
+  // (internal/fft/measure.go:89-141); later plans reuse it.
+  std::string tok;
+  if (o.planner >= GFFT_PLANNER_MEASURE && o.strategy == GFFT_KERNEL_AUTO && !wisdom_lookup(n, precision, &tok) &&
+      !variant_tokens(precision, n).empty()) {
+    const int iters = o.planner == GFFT_PLANNER_MEASURE ? 10 : o.planner == GFFT_PLANNER_PATIENT ? 50 : 100;
+    std::string best, report;
+    gfft_status ts = autotune(precision, n, 0, iters, &best, &report);
+    if (ts != GFFT_OK) {
+      delete p;
+      return ts;
+    }
+  }
+  gfft_status s = core_init(&p->core, precision, n, o.device, o.strategy);
   if (s != GFFT_OK) {
     core_free(&p->core);
     delete p;
@@ -231,6 +246,119 @@ gfft_status gfft_inverse_batch_host(gfft_plan* p, void* dst, int64_t dst_len, co
   gfft_status s = check_batch(p, dst, dst_len, src, src_len, count);
   return s != GFFT_OK ? s : run_host(p, +1, dst, src, count);
 }
+
+gfft_status gfft_plan_new_variant(gfft_plan** out, int32_t precision, int64_t n, const char* token) {
+  clear_error();
+  if (!out || !token) return GFFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (n < 1) return GFFT_ERR_INVALID_LENGTH;
+  if (precision != GFFT_COMPLEX64 && precision != GFFT_COMPLEX128) return GFFT_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
+  int dev = 0;
+  GFFT_CUDA(cudaGetDevice(&dev));
+  auto* p = new (std::nothrow) gfft_plan;
+  if (!p) return GFFT_ERR_OUT_OF_MEMORY;
+  p->opts.device = dev;
+  gfft_status s = core_init_variant(&p->core, precision, n, dev, token);
+  if (s != GFFT_OK) {
+    core_free(&p->core);
+    delete p;
+    return s;
+  }
+  *out = p;
+  return GFFT_OK;
+}
+
+static gfft_status copy_out(const std::string& text, char* buf, size_t cap, size_t* needed) {
+  if (needed) *needed = text.size() + 1;
+  if (!buf) return GFFT_OK;
+  if (cap < text.size() + 1) {
+    set_error("buffer too small");
+    return GFFT_ERR_INVALID_ARGUMENT;
+  }
+  std::memcpy(buf, text.c_str(), text.size() + 1);
+  return GFFT_OK;
+}
+
+gfft_status gfft_plan_variants(int32_t precision, int64_t n, char* buf, size_t cap, size_t* needed) {
+  clear_error();
+  std::string text;
+  for (const auto& t : variant_tokens(precision, n)) text += t + "\n";
+  return copy_out(text, buf, cap, needed);
+}
+
+gfft_status gfft_plan_check(gfft_plan* plan) {
+  clear_error();
+  if (!plan) return GFFT_ERR_INVALID_ARGUMENT;
+  if (core_device_status(&plan->core) != 0) {
+    set_error("a bounded device wait expired in this plan's kernels");
+    return GFFT_ERR_TIMEOUT;
+  }
+  return GFFT_OK;
+}
+
+gfft_status gfft_autotune(int32_t precision, int64_t n, int64_t count, int32_t iters, char* report, size_t cap,
+                          size_t* needed) {
+  clear_error();
+  if (n < 1) return GFFT_ERR_INVALID_LENGTH;
+  if (precision != GFFT_COMPLEX64 && precision != GFFT_COMPLEX128) return GFFT_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
+  std::string best, rep;
+  gfft_status s = autotune(precision, n, count, iters > 0 ? iters : 10, &best, &rep);
+  if (s != GFFT_OK) return s;
+  return copy_out(rep, report, cap, needed);
+}
+
+gfft_status gfft_wisdom_import_string(const char* text) {
+  clear_error();
+  if (!text) return GFFT_ERR_INVALID_ARGUMENT;
+  return wisdom_import(text);
+}
+
+gfft_status gfft_wisdom_export_string(char* buf, size_t cap, size_t* needed) {
+  clear_error();
+  return copy_out(wisdom_export(), buf, cap, needed);
+}
+
+gfft_status gfft_wisdom_import_file(const char* path) {
+  clear_error();
+  if (!path) return GFFT_ERR_INVALID_ARGUMENT;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    set_error(std::string("failed to open wisdom file: ") + path);
+    return GFFT_ERR_WISDOM;
+  }
+  std::string text;
+  char chunk[4096];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) text.append(chunk, got);
+  std::fclose(f);
+  return wisdom_import(text);
+}
+
+gfft_status gfft_wisdom_export_file(const char* path) {
+  clear_error();
+  if (!path) return GFFT_ERR_INVALID_ARGUMENT;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    set_error(std::string("failed to create wisdom file: ") + path);
+    return GFFT_ERR_WISDOM;
+  }
+  const std::string text = wisdom_export();
+  const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  std::fclose(f);
+  if (!ok) {
+    set_error("failed to write wisdom file");
+    return GFFT_ERR_WISDOM;
+  }
+  return GFFT_OK;
+}
+
+void gfft_wisdom_clear(void) { wisdom_clear(); }
+
+int64_t gfft_wisdom_len(void) { return int64_t(wisdom_len()); }
 
 const char* gfft_status_string(int32_t status) {
   switch (status) {

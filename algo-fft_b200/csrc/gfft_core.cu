@@ -1,9 +1,11 @@
 // Kernel registry, device twiddle generation and the 1-D schedule choice.
 #include <algorithm>
+#include <cstdio>
 #include <mutex>
 #include <vector>
 #include "gfft_internal.h"
 #include "gfft_math.cuh"
+#include "gfft_twopass.cuh"
 
 namespace gfft {
 
@@ -14,7 +16,28 @@ static std::vector<Pow2Kernel>& pow2_table() {
   return t;
 }
 
+static std::vector<TwoPassKernel>& twopass_table() {
+  static std::vector<TwoPassKernel> t;
+  return t;
+}
+
 void register_pow2(const Pow2Kernel& k) { pow2_table().push_back(k); }
+void register_twopass(const TwoPassKernel& k) { twopass_table().push_back(k); }
+
+const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te, int emax) {
+  for (const auto& k : twopass_table())
+    if (k.prec == prec && int64_t(k.n1) * k.n2 == n && k.dir == dir && (te == 0 || k.te == te) &&
+        (emax == 0 || k.emax == emax))
+      return &k;
+  return nullptr;
+}
+
+std::vector<const TwoPassKernel*> twopass_variants(int prec, int64_t n, int dir) {
+  std::vector<const TwoPassKernel*> v;
+  for (const auto& k : twopass_table())
+    if (k.prec == prec && int64_t(k.n1) * k.n2 == n && k.dir == dir) v.push_back(&k);
+  return v;
+}
 
 const Pow2Kernel* find_pow2(int prec, int n, int ept, int dir) {
   for (const auto& k : pow2_table())
@@ -44,6 +67,12 @@ cudaError_t prepare_kernels() {
       if (e != cudaSuccess) return e;
     }
   }
+  for (const auto& k : twopass_table()) {
+    if (k.smem > 48 * 1024) {
+      e = cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+      if (e != cudaSuccess) return e;
+    }
+  }
   done.push_back(dev);
   return cudaSuccess;
 }
@@ -55,30 +84,36 @@ cudaError_t prepare_kernels() {
 // and the result is accurate to a few ulp of double before rounding to the
 // element type.
 template <typename C>
-__global__ void k_twiddles(C* tw, int64_t n) {
+__global__ void k_twiddles(C* tw, int64_t n, int64_t count, int64_t step) {
   using Re = typename RealOf<C>::type;
-  for (int64_t m = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; m < n; m += int64_t(gridDim.x) * blockDim.x) {
-    int64_t mm = m;
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < count; j += int64_t(gridDim.x) * blockDim.x) {
+    int64_t mm = (j * step) % n;  // callers keep j*step < 2^62
     if (2 * mm > n) mm -= n;  // exp(-2πi m/n) == exp(-2πi (m-n)/n)
     double s, c;
     sincospi(-2.0 * double(mm) / double(n), &s, &c);
-    tw[m] = C{Re(c), Re(s)};
+    tw[j] = C{Re(c), Re(s)};
   }
+}
+
+gfft_status fill_twiddles(int prec, void* dst, int64_t n, int64_t count, int64_t step, cudaStream_t st) {
+  int blocks = int(std::min<int64_t>((count + 255) / 256, 4096));
+  if (blocks < 1) return GFFT_OK;
+  if (prec == kC64)
+    k_twiddles<float2><<<blocks, 256, 0, st>>>(static_cast<float2*>(dst), n, count, step);
+  else
+    k_twiddles<double2><<<blocks, 256, 0, st>>>(static_cast<double2*>(dst), n, count, step);
+  GFFT_CUDA(cudaGetLastError());
+  return GFFT_OK;
 }
 
 gfft_status make_twiddles(int prec, int64_t n, void** out, cudaStream_t st) {
   *out = nullptr;
   void* p = nullptr;
   GFFT_CUDA(cudaMalloc(&p, size_t(n) * elem_bytes(prec)));
-  int blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
-  if (prec == kC64)
-    k_twiddles<float2><<<blocks, 256, 0, st>>>(static_cast<float2*>(p), n);
-  else
-    k_twiddles<double2><<<blocks, 256, 0, st>>>(static_cast<double2*>(p), n);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
+  gfft_status s = fill_twiddles(prec, p, n, n, 1, st);
+  if (s != GFFT_OK) {
     cudaFree(p);
-    return cuda_status(e, "k_twiddles");
+    return s;
   }
   *out = p;
   return GFFT_OK;
@@ -116,42 +151,189 @@ static int default_ept(int prec, int64_t n) {
   return 16;
 }
 
-gfft_status core_init(PlanCore* c, int prec, int64_t n, int device) {
+static std::string twopass_token(const TwoPassKernel* k);
+
+// Two-pass plan: tables W_N1, W_N2 and the split table of W_N in one
+// allocation; slot geometry sized so the live intermediate stays in L2.
+static gfft_status init_twopass(PlanCore* c, const TwoPassKernel* f, const TwoPassKernel* inv) {
+  const int64_t n = c->n, n1 = f->n1, n2 = f->n2;
+  const size_t es = elem_bytes(c->prec);
+  int shift = (ilog2(n) + 1) / 2;
+  const int64_t nlo = int64_t(1) << shift, nhi = n >> shift;
+  GFFT_CUDA(cudaMalloc(&c->tw, size_t(n1 + n2 + nlo + nhi) * es));
+  char* base = static_cast<char*>(c->tw);
+  gfft_status s = fill_twiddles(c->prec, base, n1, n1, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + n1 * es, n2, n2, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + (n1 + n2) * es, n, nlo, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + (n1 + n2 + nlo) * es, n, nhi, nlo, 0);
+  if (s != GFFT_OK) return s;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->tp[0] = f;
+  c->tp[1] = inv;
+  c->tw1 = base;
+  c->tw2 = base + n1 * es;
+  c->bt_lo = base + (n1 + n2) * es;
+  c->bt_hi = base + (n1 + n2 + nlo) * es;
+  c->bt_shift = shift;
+  const int64_t slot_target = int64_t(8) << 20, live_target = int64_t(48) << 20;
+  const int64_t tbytes = n * int64_t(es);
+  c->group = int(std::max<int64_t>(1, slot_target / tbytes));
+  c->slots = int(std::max<int64_t>(2, std::min<int64_t>(8, live_target / (c->group * tbytes))));
+  int dev = 0, sms = 0, occ = 0;
+  GFFT_CUDA(cudaGetDevice(&dev));
+  GFFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GFFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f->func, f->tpb, f->smem));
+  c->resident = std::max(1, sms * std::max(occ, 1));
+  GFFT_CUDA(cudaMalloc(&c->status, sizeof(unsigned)));
+  GFFT_CUDA(cudaMemset(c->status, 0, sizeof(unsigned)));
+  c->algo = Algo::TwoPass;
+  c->name = twopass_token(f);
+  return GFFT_OK;
+}
+
+static std::string pow2_token(int n, int ept) {
+  return "gpu-sm100-p2-n" + std::to_string(n) + "-e" + std::to_string(ept);
+}
+
+static std::string twopass_token(const TwoPassKernel* k) {
+  return "gpu-sm100-tp-" + std::to_string(k->n1) + "x" + std::to_string(k->n2) + "-t" + std::to_string(k->te) +
+         "-e" + std::to_string(k->emax);
+}
+
+std::vector<std::string> variant_tokens(int prec, int64_t n) {
+  std::vector<std::string> v;
+  if (n > 1 && (n & (n - 1)) == 0) {
+    if (n <= (prec == kC64 ? 16384 : 8192))
+      for (const Pow2Kernel* k : pow2_variants(prec, int(n), -1)) v.push_back(pow2_token(k->n, k->ept));
+    for (const TwoPassKernel* k : twopass_variants(prec, n, -1)) v.push_back(twopass_token(k));
+  }
+  return v;
+}
+
+static gfft_status init_pow2(PlanCore* c, int ept) {
+  const Pow2Kernel* f = find_pow2(c->prec, int(c->n), ept, -1);
+  const Pow2Kernel* i = find_pow2(c->prec, int(c->n), ept, +1);
+  if (!f || !i) {
+    set_error("no compiled power-of-two kernel for this size");
+    return GFFT_ERR_NOT_IMPLEMENTED;
+  }
+  c->algo = Algo::Pow2Smem;
+  c->k[0] = f;
+  c->k[1] = i;
+  gfft_status s = make_twiddles(c->prec, c->n, &c->tw, 0);
+  if (s != GFFT_OK) return s;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->name = pow2_token(int(c->n), ept);
+  return GFFT_OK;
+}
+
+gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, const std::string& tok) {
+  c->prec = prec;
+  c->n = n;
+  c->device = device;
+  GFFT_CUDA(prepare_kernels());
+  int a = 0, b = 0, te = 0, e = 0;
+  if (std::sscanf(tok.c_str(), "gpu-sm100-p2-n%d-e%d", &a, &e) == 2 && a == n) return init_pow2(c, e);
+  if (std::sscanf(tok.c_str(), "gpu-sm100-tp-%dx%d-t%d-e%d", &a, &b, &te, &e) == 4 && int64_t(a) * b == n) {
+    const TwoPassKernel* f = find_twopass(prec, n, -1, te, e);
+    const TwoPassKernel* i = find_twopass(prec, n, +1, te, e);
+    if (f && i) return init_twopass(c, f, i);
+  }
+  set_error("unknown or uncompiled variant '" + tok + "' for length " + std::to_string(n));
+  return GFFT_ERR_INVALID_ARGUMENT;
+}
+
+gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy) {
   c->prec = prec;
   c->n = n;
   c->device = device;
   if (n == 1) {
     c->algo = Algo::Trivial;
-    c->name = "gpu:sm100:copy:n1";
+    c->name = "gpu-sm100-copy-n1";
     return GFFT_OK;
   }
   GFFT_CUDA(prepare_kernels());
   const bool pow2 = (n & (n - 1)) == 0;
   const int64_t max_single = prec == kC64 ? 16384 : 8192;
-  if (pow2 && n <= max_single) {
-    int ept = default_ept(prec, n);
-    const Pow2Kernel* f = find_pow2(prec, int(n), ept, -1);
-    const Pow2Kernel* i = find_pow2(prec, int(n), ept, +1);
-    if (!f || !i) {
-      set_error("no compiled power-of-two kernel for this size");
-      return GFFT_ERR_NOT_IMPLEMENTED;
-    }
-    c->algo = Algo::Pow2Smem;
-    c->k[0] = f;
-    c->k[1] = i;
-    gfft_status s = make_twiddles(prec, n, &c->tw, 0);
-    if (s != GFFT_OK) return s;
-    GFFT_CUDA(cudaStreamSynchronize(0));
-    c->name = "gpu:sm100:pow2:n" + std::to_string(n) + ":ept" + std::to_string(ept);
-    return GFFT_OK;
+  // A forced strategy (SetKernelStrategy / PlanOptions.Strategy,
+  // internal/planner/selection.go:71-78) picks the schedule class: the
+  // step kernels map to the two-pass schedule, DIT/Stockham to the
+  // single-pass one; a class that cannot serve n falls back to auto.
+  const bool want_twopass = strategy == GFFT_KERNEL_SIXSTEP || strategy == GFFT_KERNEL_EIGHTSTEP;
+  const bool want_single = strategy == GFFT_KERNEL_DIT || strategy == GFFT_KERNEL_STOCKHAM;
+  if (strategy == GFFT_KERNEL_AUTO) {
+    std::string tok;
+    if (wisdom_lookup(n, prec, &tok) && core_init_variant(c, prec, n, device, tok) == GFFT_OK) return GFFT_OK;
+    clear_error();
+  }
+  if (pow2 && n <= max_single && !want_twopass) return init_pow2(c, default_ept(prec, n));
+  if (pow2 && !want_single) {
+    const TwoPassKernel* f = find_twopass(prec, n, -1, prec == kC64 ? 8192 : 4096, prec == kC64 ? 16 : 8);
+    const TwoPassKernel* i = find_twopass(prec, n, +1, prec == kC64 ? 8192 : 4096, prec == kC64 ? 16 : 8);
+    if (f && i) return init_twopass(c, f, i);
+  }
+  if (pow2 && n <= max_single) return init_pow2(c, default_ept(prec, n));
+  if (pow2) {
+    const TwoPassKernel* f = find_twopass(prec, n, -1);
+    const TwoPassKernel* i = find_twopass(prec, n, +1);
+    if (f && i) return init_twopass(c, f, i);
   }
   set_error("length " + std::to_string(n) + " has no GPU schedule yet");
   return GFFT_ERR_NOT_IMPLEMENTED;
 }
 
+unsigned core_device_status(const PlanCore* c) {
+  if (!c->status) return 0;
+  unsigned v = 0;
+  if (cudaMemcpy(&v, c->status, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+  return v;
+}
+
 void core_free(PlanCore* c) {
-  if (c->tw) cudaFree(c->tw);
-  c->tw = nullptr;
+  for (void** p : {&c->tw, reinterpret_cast<void**>(&c->status)}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+}
+
+static gfft_status exec_twopass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                                int64_t idist, int64_t odist, cudaStream_t st) {
+  const TwoPassKernel* k = c->tp[dir < 0 ? 0 : 1];
+  const size_t es = elem_bytes(c->prec);
+  const int groups = int((count + c->group - 1) / c->group);
+  const size_t ctr_bytes = (size_t(1) + 2 * size_t(groups)) * sizeof(unsigned);
+  const size_t ctr_pad = (ctr_bytes + 255) & ~size_t(255);
+  const size_t scratch_bytes = size_t(c->slots) * size_t(c->group) * size_t(c->n) * es;
+  void* ws = nullptr;
+  GFFT_CUDA(cudaMallocAsync(&ws, ctr_pad + scratch_bytes, st));
+  cudaError_t e = cudaMemsetAsync(ws, 0, ctr_bytes, st);
+  if (e == cudaSuccess) {
+    TwoPassParams p;
+    p.src = src;
+    p.dst = dst;
+    p.scratch = static_cast<char*>(ws) + ctr_pad;
+    p.count = count;
+    p.idist = idist;
+    p.odist = odist;
+    p.tw1 = c->tw1;
+    p.tw2 = c->tw2;
+    p.bt.lo = c->bt_lo;
+    p.bt.hi = c->bt_hi;
+    p.bt.shift = c->bt_shift;
+    p.ctr = static_cast<unsigned*>(ws);
+    p.status = c->status;
+    p.groups = groups;
+    p.G = c->group;
+    p.S = c->slots;
+    p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+    p.spin_limit = 1u << 24;
+    const int64_t tiles = int64_t(groups) * c->group * ((k->n2 / k->nc1) + (k->n1 / k->nc2));
+    const int grid = int(std::min<int64_t>(tiles, c->resident));
+    e = k->launch(p, grid, st);
+  }
+  cudaFreeAsync(ws, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_twopass");
+  return GFFT_OK;
 }
 
 gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
@@ -170,6 +352,8 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
       GFFT_CUDA(cudaGetLastError());
       return GFFT_OK;
     }
+    case Algo::TwoPass:
+      return exec_twopass(c, dir, dst, src, count, idist, odist, st);
     case Algo::Pow2Smem: {
       const Pow2Kernel* k = c->k[dir < 0 ? 0 : 1];
       const double scale = dir < 0 ? 1.0 : 1.0 / double(c->n);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 #include "../../include/gfft.h"
 #include "gfft_registry.h"
 
@@ -19,7 +20,7 @@ gfft_status cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::gfft::cuda_status(e_, #call); \
   } while (0)
 
-enum class Algo { Trivial, Pow2Smem };
+enum class Algo { Trivial, Pow2Smem, TwoPass };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
 // FP64 and rounded to the element type (internal/math/twiddle.go:8-21).
@@ -31,13 +32,42 @@ struct PlanCore {
   int device = 0;
   Algo algo = Algo::Trivial;
   const Pow2Kernel* k[2] = {nullptr, nullptr};  // [0] forward, [1] inverse
-  void* tw = nullptr;
+  void* tw = nullptr;                            // twiddle tables (one allocation)
   std::string name;
+  // two-pass schedule
+  const TwoPassKernel* tp[2] = {nullptr, nullptr};
+  const void* tw1 = nullptr;                     // W_N1
+  const void* tw2 = nullptr;                     // W_N2
+  const void* bt_lo = nullptr;
+  const void* bt_hi = nullptr;
+  int bt_shift = 0;
+  int group = 1, slots = 2, resident = 1;
+  unsigned* status = nullptr;  // device word: nonzero once a bounded wait expired
 };
 
-// Chooses and prepares the schedule of a 1-D complex transform of length n.
-gfft_status core_init(PlanCore* c, int prec, int64_t n, int device);
+// Fills dst[j] = W_n^{(j*step) mod n} for j < count (FP64, rounded).
+gfft_status fill_twiddles(int prec, void* dst, int64_t n, int64_t count, int64_t step, cudaStream_t st);
+
+// Chooses and prepares the schedule of a 1-D complex transform of length n:
+// a forced strategy class, else the wisdom store's variant, else defaults.
+gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy = GFFT_KERNEL_AUTO);
+// Prepares the exact kernel variant named by a wisdom token.
+gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, const std::string& token);
 void core_free(PlanCore* c);
+// Nonzero once a bounded device wait of this plan expired (synchronous read).
+unsigned core_device_status(const PlanCore* c);
+// Tokens of every compiled variant that can compute length n.
+std::vector<std::string> variant_tokens(int prec, int64_t n);
+
+// Wisdom store (process-wide).
+bool wisdom_lookup(int64_t n, int prec, std::string* algo);
+void wisdom_store(int64_t n, int prec, const std::string& algo);
+gfft_status wisdom_import(const std::string& text);
+std::string wisdom_export();
+void wisdom_clear();
+size_t wisdom_len();
+// Times every variant of length n on count transforms; records the fastest.
+gfft_status autotune(int prec, int64_t n, int64_t count, int iters, std::string* best, std::string* report);
 
 // Runs `count` transforms (dir -1 forward, +1 inverse) with element strides
 // idist/odist between consecutive transforms; device pointers.

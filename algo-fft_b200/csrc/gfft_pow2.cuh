@@ -3,20 +3,22 @@
 // One transform is owned by T = N/EPT threads; each thread holds EPT
 // elements in registers.  Stage s (radix RS, p = product of the previous
 // radices) is Stockham's self-sorting step: butterfly i reads
-// x[i + r*N/RS], multiplies by W_{p*RS}^{r*k} (k = i mod p), runs DFT_RS in
-// registers and writes y[(i-k)*RS + k + r*p].  The first stage reads
-// straight from HBM and the last writes straight to HBM, both at unit
-// stride across the T threads (fully coalesced), so shared memory carries
-// only the exchanges in between.  Shared memory is padded by one element
-// every EPT elements, which makes every exchange pattern bank-conflict free
-// for EPT >= 8 (checked exhaustively on the CPU for each schedule).
+// x[i + r*N/RS], multiplies by W_{p*RS}^{r*k} (k = i mod p; one coalesced
+// load of W_{p*RS}^k, powers by a product tree), runs DFT_RS in registers
+// and writes y[(i-k)*RS + k + r*p].  The first stage reads straight from HBM and the last writes straight to HBM,
+// both at unit stride across the T threads (fully coalesced), so shared
+// memory carries only the exchanges in between.  Shared memory is padded by
+// one element every EPT elements, which makes every exchange pattern
+// bank-conflict free for EPT >= 8 (checked exhaustively on the CPU for each
+// schedule), and keeps every shared address of a thread a compile-time
+// offset from one base per butterfly.
 //
 // Replaces the reference's size-specific DIT codelets 4..16384
 // (internal/kernels/codelet_init.go:60-440) and the radix-2 Stockham
 // (internal/kernels/stockham.go:21) for one batch of transforms
 // (plan.go:504-571).
 #pragma once
-#include "gfft_math.cuh"
+#include "gfft_sched.cuh"
 
 namespace gfft {
 
@@ -43,8 +45,9 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
                                            const C* __restrict__ tw,
                                            typename RealOf<C>::type scale) {
   using S = Pow2Shape<N, EPT, sizeof(C)>;
+  using SC = Sched<N, EPT>;
   constexpr int T = S::T;
-  constexpr int RS = (P * EPT <= N) ? EPT : N / P;
+  constexpr int RS = SC::radix_at(P);
   constexpr int Q = EPT / RS;
   constexpr int STRIDE = N / RS;
   constexpr bool FIRST = (P == 1);
@@ -54,22 +57,25 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
-      for (int r = 0; r < RS; ++r) {
-        const int e = t + q * T + r * STRIDE;
-        v[q * RS + r] = valid ? ld_stream(in + e) : C{0, 0};
-      }
+      for (int r = 0; r < RS; ++r) v[q * RS + r] = valid ? ld_stream(in + (t + q * T + r * STRIDE)) : C{0, 0};
   } else {
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
+    for (int q = 0; q < Q; ++q) {
+      if constexpr (STRIDE % EPT == 0) {
+        const int pb = S::pad(t + q * T);
 #pragma unroll
-      for (int r = 0; r < RS; ++r) v[q * RS + r] = sh[S::pad(t + q * T + r * STRIDE)];
+        for (int r = 0; r < RS; ++r) v[q * RS + r] = sh[pb + r * (STRIDE + STRIDE / EPT)];
+      } else {
+#pragma unroll
+        for (int r = 0; r < RS; ++r) v[q * RS + r] = sh[S::pad(t + q * T + r * STRIDE)];
+      }
+    }
   }
 
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     if constexpr (P > 1) {
-      const int i = t + q * T;
-      const int k = i & (P - 1);
+      const int k = (t + q * T) & (P - 1);
       apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + k * (N / (P * RS))));
     }
     dft<RS, DIR>(v + q * RS);
@@ -81,8 +87,9 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int r = 0; r < RS; ++r) {
-          const int e = t + q * T + r * P;
-          st_stream(out + e, cscale(v[q * RS + r], scale));
+          C o = v[q * RS + r];
+          if constexpr (DIR > 0) o = cscale(o, scale);
+          st_stream(out + (t + q * T + r * P), o);
         }
     }
   } else {
@@ -91,9 +98,17 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
     for (int q = 0; q < Q; ++q) {
       const int i = t + q * T;
       const int k = i & (P - 1);
-      const int j = (i - k) * RS + k;
+      const int a = i / P;
+      // pad(j + r*P) with j = a*P*RS + k: every term but the last is per-butterfly.
+      const int jb = a * P * RS + k + (a * P * RS) / EPT;
+      if constexpr (P >= EPT) {
+        const int pb = jb + (k >> S::PSH);
 #pragma unroll
-      for (int r = 0; r < RS; ++r) sh[S::pad(j + r * P)] = v[q * RS + r];
+        for (int r = 0; r < RS; ++r) sh[pb + r * (P + P / EPT)] = v[q * RS + r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < RS; ++r) sh[jb + r * P + r / (EPT / P)] = v[q * RS + r];
+      }
     }
     xsync<T>();
     pow2_stage<C, N, EPT, DIR, P * RS>(v, in, out, sh, t, valid, tw, scale);
@@ -102,7 +117,7 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
 
 // Batched C2C: transform b reads src[b*idist .. b*idist+N) and writes
 // dst[b*odist ..).  src may equal dst (every CTA reads its whole transform
-// before it writes any of it).  tw holds W_N^m, m < N, in the element type.
+// before it writes any of it).  tw holds W_N^m, m < N.
 template <typename C, int N, int EPT, int DIR>
 __global__ void __launch_bounds__(Pow2Shape<N, EPT, sizeof(C)>::TPB)
 k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const C* __restrict__ tw,

@@ -9,6 +9,7 @@ namespace gfft {
 
 enum Prec { kC64 = 0, kC128 = 1 };
 
+
 // Single-pass power-of-two kernel (k_pow2) of one (precision, N, EPT, dir).
 struct Pow2Kernel {
   int prec, n, ept, dir;
@@ -20,7 +21,21 @@ struct Pow2Kernel {
                         const void* tw, double scale, cudaStream_t st);
 };
 
+// Persistent two-pass kernel (k_twopass) of one (precision, N1 x N2, dir).
+struct TwoPassParams;
+struct TwoPassKernel {
+  int prec, n1, n2, dir;
+  int tpb, smem;
+  int nc1, nc2;   // columns per tile in pass 1 / pass 2
+  int te = 0, emax = 0;  // variant: tile elements, max elements per thread
+  const void* func;
+  cudaError_t (*launch)(const TwoPassParams& p, int grid, cudaStream_t st);
+};
+
 void register_pow2(const Pow2Kernel& k);
+void register_twopass(const TwoPassKernel& k);
+const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te = 0, int emax = 0);
+std::vector<const TwoPassKernel*> twopass_variants(int prec, int64_t n, int dir);
 const Pow2Kernel* find_pow2(int prec, int n, int ept, int dir);
 std::vector<const Pow2Kernel*> pow2_variants(int prec, int n, int dir);
 

@@ -1,0 +1,313 @@
+// Two-pass (four-step) transform for large N = N1 * N2 (K2), as one
+// persistent kernel that keeps the intermediate in L2.
+//
+// Index maps: n = N2*n1 + n2 (input), k = k1 + N1*k2 (output).
+//   pass 1: for each column n2, FFT_N1 over n1 of x[N2*n1 + n2], multiply by
+//           W_N^{n2*k1}, store transposed: Y[n2][k1] (rows of N1, scratch).
+//   pass 2: for each k1, FFT_N2 over n2 of Y[n2][k1] (a column of Y), store
+//           X[k1 + N1*k2] (a column of the output viewed as N2 x N1).
+// A tile is NC adjacent columns of one transform, so every global access is
+// a run of NC contiguous elements (pass 1's store is a run of N1).
+//
+// Scheduling: the batch is cut into groups of G transforms; each group's
+// intermediate lives in one of S scratch slots small enough to stay in the
+// 126 MB L2, so HBM sees one read of the input and one write of the output.
+// Persistent CTAs take tiles from a global counter in a fixed order
+//   P1(0..S-2), then P2(k), P1(k+S-1) for k = 0, 1, ...
+// A pass-2 tile of group g waits (bounded) until all pass-1 tiles of g are
+// done; a pass-1 tile of group g >= S waits until pass 2 of g-S has released
+// its slot.  Every wait targets tiles handed out earlier, which are held by
+// running CTAs whose own waits target still earlier tiles, so the chain
+// always ends: no deadlock, whatever the residency.  Waits are bounded
+// anyway: on expiry the kernel records an error and returns.
+//
+// Replaces the reference's six-step / eight-step kernels
+// (internal/kernels/sixstep.go:29-91, eightstep.go:27-154) and the packed
+// Stockham for large power-of-two N (internal/transform/stockham_packed.go:86).
+#pragma once
+#include "gfft_pow2.cuh"
+#include "gfft_sched.cuh"
+
+namespace gfft {
+
+// Tile of NC columns of length L, EPT elements per thread.
+template <int L, int EPT, int NC, int ES>
+struct ColShape {
+  static_assert((NC & (NC - 1)) == 0, "NC must be a power of two");
+  static constexpr int T = L / EPT;     // threads per column
+  static constexpr int TPB = T * NC;    // threads per tile
+  // Rows of NC+1 elements when NC >= 16 (odd pitch: row-wise and column-wise
+  // accesses are both bank-conflict free); narrower tiles use an XOR swizzle
+  // of the column index by the row, which keeps most of that property.
+  static constexpr bool PITCHED = NC >= 16;
+  static constexpr int PITCH = PITCHED ? NC + 1 : NC;
+  static constexpr int SMEM = L * PITCH * ES;
+  __device__ static __forceinline__ int phys(int row, int c) {
+    if constexpr (PITCHED) return row * PITCH + c;
+    else return row * NC + (c ^ (row & (NC - 1)));
+  }
+};
+
+struct BigTwiddle {
+  const void* lo;  // W_N^j, j < 2^shift
+  const void* hi;  // W_N^(j << shift), j < N >> shift
+  int shift;
+};
+
+template <typename C, int DIR>
+__device__ __forceinline__ C big_twiddle(const BigTwiddle& bt, int64_t m) {
+  const C* lo = static_cast<const C*>(bt.lo);
+  const C* hi = static_cast<const C*>(bt.hi);
+  C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & ((int64_t(1) << bt.shift) - 1))));
+  if constexpr (DIR > 0) w.y = -w.y;
+  return w;
+}
+
+enum { LOAD_STREAM = 0, LOAD_L2 = 1 };
+enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1 };
+
+template <int LOADK, typename C>
+__device__ __forceinline__ C gload(const C* p) {
+  if constexpr (LOADK == LOAD_L2) return __ldcg(p);
+  else return ld_stream(p);
+}
+
+// One Stockham stage of a column tile (see pow2_stage for the algebra).
+// Element (row, c) of the tile lives at sh[phys(row, c)]; global row r of
+// column c is at in[r*istride + c].
+template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE>
+__device__ __forceinline__ void col_stage(C* v, const C* in, int64_t istride, C* out, int64_t ostride, C* sh,
+                                          int t, int c, bool active, const C* __restrict__ tw,
+                                          typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2) {
+  using S = ColShape<L, EPT, NC, sizeof(C)>;
+  using SC = Sched<L, EPT>;
+  constexpr int T = S::T;
+  constexpr int RS = SC::radix_at(P);
+  constexpr int Q = EPT / RS;
+  constexpr int STRIDE = L / RS;
+  constexpr bool FIRST = (P == 1);
+  constexpr bool LAST = (P * RS == L);
+
+  if (active) {
+    if constexpr (FIRST) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r)
+          v[q * RS + r] = gload<LOADK>(in + int64_t(t + q * T + r * STRIDE) * istride + c);
+    } else {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) v[q * RS + r] = sh[S::phys(t + q * T + r * STRIDE, c)];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if constexpr (P > 1) {
+        const int k = (t + q * T) & (P - 1);
+        apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + k * (L / (P * RS))));
+      }
+      dft<RS, DIR>(v + q * RS);
+    }
+  }
+
+  if constexpr (LAST && MODE == OUT_COLUMNS) {
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) {
+          C o = v[q * RS + r];
+          if constexpr (DIR > 0) o = cscale(o, scale);
+          st_stream(out + int64_t(t + q * T + r * P) * ostride + c, o);
+        }
+    }
+  } else if constexpr (LAST) {
+    if constexpr (!FIRST) __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int row0 = t + q * T;
+        const int64_t m0 = n2 * row0, dm = n2 * P;
+#pragma unroll
+        for (int r = 0; r < RS; ++r)
+          sh[S::phys(row0 + r * P, c)] = cmul(v[q * RS + r], big_twiddle<C, DIR>(bt, m0 + r * dm));
+      }
+    }
+    __syncthreads();
+  } else {
+    if constexpr (!FIRST) __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int i = t + q * T;
+        const int k = i & (P - 1);
+        const int j = (i - k) * RS + k;
+#pragma unroll
+        for (int r = 0; r < RS; ++r) sh[S::phys(j + r * P, c)] = v[q * RS + r];
+      }
+    }
+    __syncthreads();
+    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE>(v, in, istride, out, ostride, sh, t, c, active, tw, scale,
+                                                       bt, n2);
+  }
+}
+
+struct TwoPassParams {
+  const void* src;
+  void* dst;
+  void* scratch;       // S slots of G*N elements
+  int64_t count, idist, odist;
+  const void* tw1;     // W_N1^m, m < N1
+  const void* tw2;     // W_N2^m, m < N2
+  BigTwiddle bt;       // W_N^m
+  unsigned* ctr;       // [0] next tile, [1 + g] pass-1 done, [1 + groups + g] pass-2 done
+  unsigned* status;    // 0 ok, 1 a bounded wait expired
+  int groups, G, S;
+  double scale;        // applied in pass 2 (1/N for the inverse)
+  unsigned spin_limit;
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded wait of one thread for *p >= target.
+__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned target, unsigned limit) {
+  unsigned it = 0;
+  while (ld_acquire(p) < target) {
+    if (++it > limit) return false;
+    __nanosleep(128);
+  }
+  return true;
+}
+
+template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int DIR>
+struct TwoPass {
+  using S1 = ColShape<N1, EPT1, NC1, sizeof(C)>;
+  using S2 = ColShape<N2, EPT2, NC2, sizeof(C)>;
+  static constexpr int64_t N = int64_t(N1) * N2;
+  static constexpr int TILES1 = N2 / NC1;  // pass-1 tiles per transform
+  static constexpr int TILES2 = N1 / NC2;  // pass-2 tiles per transform
+  static constexpr int TPB = S1::TPB > S2::TPB ? S1::TPB : S2::TPB;
+  static constexpr int SMEM = S1::SMEM > S2::SMEM ? S1::SMEM : S2::SMEM;
+  static constexpr int EPT = EPT1 > EPT2 ? EPT1 : EPT2;
+  // resident CTAs per SM the register allocation must allow (smem-bound)
+  static constexpr int MB0 = (200 * 1024) / (SMEM > 0 ? SMEM : 1);
+  static constexpr int MIN_BLOCKS = MB0 < 1 ? 1 : (MB0 > 4 ? 4 : MB0);
+};
+
+// Tile order decode (see the header comment).
+__device__ __forceinline__ void decode_tile(int64_t w, int groups, int S, int64_t T1, int64_t T2, int& pass,
+                                            int& g, int64_t& tile) {
+  const int64_t init = groups < S - 1 ? groups : S - 1;
+  if (w < init * T1) {
+    pass = 1;
+    g = int(w / T1);
+    tile = w % T1;
+    return;
+  }
+  w -= init * T1;
+  const int64_t k1 = groups - (S - 1) > 0 ? groups - (S - 1) : 0;  // pairs that carry a pass-1 unit
+  if (w < k1 * (T1 + T2)) {
+    const int64_t k = w / (T1 + T2), rem = w % (T1 + T2);
+    if (rem < T2) {
+      pass = 2;
+      g = int(k);
+      tile = rem;
+    } else {
+      pass = 1;
+      g = int(k + S - 1);
+      tile = rem - T2;
+    }
+    return;
+  }
+  w -= k1 * (T1 + T2);
+  pass = 2;
+  g = int(k1 + w / T2);
+  tile = w % T2;
+}
+
+template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int DIR>
+__global__ void __launch_bounds__(TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>::TPB,
+                                  TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>::MIN_BLOCKS)
+k_twopass(TwoPassParams p) {
+  using TP = TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
+  using S1 = typename TP::S1;
+  using S2 = typename TP::S2;
+  using Re = typename RealOf<C>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw);
+  __shared__ int64_t s_w;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x;
+  const int64_t T1 = int64_t(TP::TILES1) * p.G, T2 = int64_t(TP::TILES2) * p.G;
+  const int64_t total = int64_t(p.groups) * (T1 + T2);
+  const C* src = static_cast<const C*>(p.src);
+  C* dst = static_cast<C*>(p.dst);
+  C* scratch = static_cast<C*>(p.scratch);
+  unsigned* done1 = p.ctr + 1;
+  unsigned* done2 = p.ctr + 1 + p.groups;
+  C v[TP::EPT];
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) {
+      s_w = (ld_acquire(p.status) != 0) ? total : int64_t(atomicAdd(p.ctr, 1u));
+    }
+    __syncthreads();
+    const int64_t w = s_w;
+    if (w >= total) break;
+    int pass, g;
+    int64_t tile;
+    decode_tile(w, p.groups, p.S, T1, T2, pass, g, tile);
+    if (tid == 0) {
+      bool ok = true;
+      if (pass == 2) ok = wait_at_least(done1 + g, unsigned(T1), p.spin_limit);
+      else if (g >= p.S) ok = wait_at_least(done2 + (g - p.S), unsigned(T2), p.spin_limit);
+      if (!ok) atomicExch(p.status, 1u);
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) break;
+    const int slot = g % p.S;
+    if (pass == 1) {
+      const int64_t b = int64_t(g) * p.G + tile / TP::TILES1;  // transform index
+      const int col0 = int(tile % TP::TILES1) * NC1;
+      const bool valid = b < p.count;
+      const bool active = valid && tid < S1::TPB;
+      const int c = tid % NC1, t = tid / NC1;
+      const C* in = src + (valid ? b * p.idist : 0) + col0;
+      C* y = scratch + (int64_t(slot) * p.G + (b - int64_t(g) * p.G)) * TP::N;
+      col_stage<C, N1, EPT1, NC1, DIR, 1, LOAD_STREAM, OUT_SMEM_TWIDDLE>(
+          v, in, N2, nullptr, 0, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c));
+      if (valid) {
+        // transposed store: Y[col0 + cc][row], rows of N1 contiguous
+        for (int e = tid; e < N1 * NC1; e += TP::TPB) {
+          const int cc = e / N1, row = e % N1;
+          __stcg(y + int64_t(col0 + cc) * N1 + row, sh[S1::phys(row, cc)]);
+        }
+      }
+    } else {
+      const int64_t b = int64_t(g) * p.G + tile / TP::TILES2;
+      const int col0 = int(tile % TP::TILES2) * NC2;
+      const bool valid = b < p.count;
+      const bool active = valid && tid < S2::TPB;
+      const int c = tid % NC2, t = tid / NC2;
+      const C* y = scratch + (int64_t(slot) * p.G + (b - int64_t(g) * p.G)) * TP::N + col0;
+      C* out = dst + (valid ? b * p.odist : 0) + col0;
+      col_stage<C, N2, EPT2, NC2, DIR, 1, LOAD_L2, OUT_COLUMNS>(v, y, N1, out, N1, sh, t, c, active,
+                                                                static_cast<const C*>(p.tw2), Re(p.scale),
+                                                                p.bt, 0);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(pass == 1 ? done1 + g : done2 + g, 1u);
+    }
+  }
+}
+
+}  // namespace gfft

@@ -32,8 +32,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "algo-fft_b200"))
 
 BUF_BYTES = 1 << 30                      # one 1 GiB batch per length
-SWEEP = [2 ** k for k in range(10, 15)]  # lengths with a single-pass schedule
-WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^10..2^14, 1 GiB batch per N"
+SWEEP = [2 ** k for k in range(10, 25)]
+WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^10..2^24, 1 GiB batch per N"
 
 
 def bytes_per_transform(n: int) -> int:
@@ -67,9 +67,16 @@ class ClockSampler:
                                        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self._p.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self._p = None
         return self
+
+    def mark(self):
+        """Index of the first sample taken after this call."""
+        return len(self.rows)
 
     def _read(self):
         for line in self._p.stdout:
@@ -85,15 +92,16 @@ class ClockSampler:
             except Exception:
                 self._p.kill()
 
-    def summary(self):
-        if not self.rows:
+    def summary(self, since: int = 0):
+        rows = self.rows[since:] or self.rows
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def dist_setup(args):
@@ -114,7 +122,7 @@ def cpu_baseline(sample_seconds: float = 12.0):
     total_bytes, total_t, sample = 0, 0.0, []
     rng = np.random.default_rng(0)
     for n in SWEEP:
-        count = max(threads, (1 << 22) // n)
+        count = max(1, min(max(threads, (1 << 22) // n), (1 << 25) // n))
         x = (rng.standard_normal(n * count) + 1j * rng.standard_normal(n * count)).astype(np.complex64)
         t0 = time.perf_counter()
         oracle.batch(x, n, nthreads=threads)
@@ -153,12 +161,16 @@ def run_reference(args):
 
 
 def main():
+    global SWEEP, BUF_BYTES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-slice leg (profiling runs)")
+    ap.add_argument("--sizes", default="", help="comma-separated subset of lengths (profiling runs)")
+    ap.add_argument("--batch-mib", type=int, default=BUF_BYTES >> 20, help="batch bytes per length in MiB")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -167,6 +179,9 @@ def main():
     import torch
     import algofft
 
+    if args.sizes:
+        SWEEP = [int(v) for v in args.sizes.split(",")]
+    BUF_BYTES = args.batch_mib << 20
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
     pg = None
@@ -181,11 +196,13 @@ def main():
     plans, bufs = {}, {}
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234 + rank)
+    # one 1 GiB input and one 1 GiB output, viewed as count x N for every N
+    xin = torch.randn(BUF_BYTES // 4, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+    yout = torch.empty_like(xin)
     for n in SWEEP:
         count = BUF_BYTES // (8 * n)
         plans[n] = algofft.NewPlan(n)
-        x = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
-        bufs[n] = (x, torch.empty_like(x), count)
+        bufs[n] = (xin, yout, count)
 
     def step(evs=None):
         for i, n in enumerate(SWEEP):
@@ -194,6 +211,7 @@ def main():
             if evs is not None:
                 evs[i].record(stream)
 
+    clk = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -203,7 +221,8 @@ def main():
     per_size_ms = {n: 0.0 for n in SWEEP}
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    mark = clk.mark()
+    if True:
         torch.cuda.synchronize()
         start.record(stream)
         for s in range(args.steps):
@@ -218,6 +237,8 @@ def main():
                 prev = evs[i]
         end.record(stream)
         torch.cuda.synchronize()
+    time.sleep(0.3)
+    clk.__exit__()
     total_ms = start.elapsed_time(end)
     dev_ms = sum(per_size_ms.values())  # kernels only (host gaps between steps excluded)
     t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
@@ -238,24 +259,23 @@ def main():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     errs = {}
-    for n in SWEEP:
+    for n in SWEEP:  # the shared output holds the last length's result: rerun each length once
         x, y, count = bufs[n]
-        xs = x[: n * 2].cpu().numpy().astype(np.complex128)
-        ys = y[: n * 2].cpu().numpy().astype(np.complex128)
+        plans[n].ForwardBatch(y, x, count)
+        torch.cuda.synchronize()
+        xs = x[: n].cpu().numpy().astype(np.complex128)
+        ys = y[: n].cpu().numpy().astype(np.complex128)
         ref = oracle.batch(xs, n)
         errs[n] = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
     # end to end: the same sweep through the host-slice API (pinned host
     # buffers, H2D + transform + D2H inside the timed region, every step)
-    e2e_steps = max(1, min(args.steps, 3))
-    host = {}
-    for n in SWEEP:
-        x, y, count = bufs[n]
-        hx = torch.empty(x.numel(), dtype=torch.complex64, pin_memory=True)
-        hx.copy_(x)
-        hy = torch.empty_like(hx, pin_memory=True)
-        host[n] = (hx.numpy(), hy.numpy(), count)
-    for n in SWEEP:  # warm the staging pool
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    hx_t = torch.empty(xin.numel(), dtype=torch.complex64, pin_memory=True)
+    hx_t.copy_(xin)
+    hy_t = torch.empty_like(hx_t, pin_memory=True)
+    host = {n: (hx_t.numpy(), hy_t.numpy(), bufs[n][2]) for n in SWEEP}
+    for n in SWEEP if e2e_steps else []:  # warm the staging pool
         hx, hy, count = host[n]
         plans[n].ForwardBatch(hy, hx, count)
     if pg:
@@ -269,7 +289,7 @@ def main():
     te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
     if pg:
         pg.all_reduce(te, op=pg.ReduceOp.MAX)
-    e2e_val = world * bytes_step * e2e_steps / float(te.item()) / 1e9
+    e2e_val = world * bytes_step * e2e_steps / max(float(te.item()), 1e-9) / 1e9
 
     if rank == 0:
         line = {
@@ -287,7 +307,7 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": None,
                          "algorithmic_bytes_per_launch": dom_bytes},
-            "clocks": clk.summary(),
+            "clocks": clk.summary(mark),
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": bytes_step // 2,
                     "d2h_bytes_per_step": bytes_step // 2, "steps": e2e_steps,
                     "path": "Plan.ForwardBatch on pinned host slices (gfft_forward_batch_host)"},

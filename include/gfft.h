@@ -103,6 +103,43 @@ GFFT_API int64_t gfft_plan_len(const gfft_plan* plan);
  * NUL-terminated string, e.g. "gpu:sm100:pow2:n1024:ept32". */
 GFFT_API gfft_status gfft_plan_algorithm(const gfft_plan* plan, char* buf, size_t cap);
 
+/* Creates a plan bound to one compiled kernel variant named by a wisdom
+ * token (as listed by gfft_plan_variants), bypassing the planner: the
+ * forced-strategy path of SetKernelStrategy (internal/planner/selection.go:22-29)
+ * at kernel granularity. */
+GFFT_API gfft_status gfft_plan_new_variant(gfft_plan** out, int32_t precision, int64_t n, const char* token);
+
+/* Newline-separated tokens of every compiled variant for (precision, n).
+ * With buf == NULL only *needed (bytes incl. NUL) is set. */
+GFFT_API gfft_status gfft_plan_variants(int32_t precision, int64_t n, char* buf, size_t cap, size_t* needed);
+
+/* Returns GFFT_ERR_TIMEOUT if a bounded device wait in this plan's kernels
+ * has expired (the kernels then stop early and set a device flag instead of
+ * hanging); synchronous. */
+GFFT_API gfft_status gfft_plan_check(gfft_plan* plan);
+
+/* ---- planner: autotuner and wisdom (wisdom.go:13-82, measure.go:89-228) ---- */
+
+/* MeasureAndSelect (internal/fft/measure.go:89-141) on the GPU: times every
+ * compiled variant of length n on `count` transforms (0 = about 2^25
+ * elements) with CUDA events, `iters` timed runs each (median), records the
+ * fastest in the wisdom store and writes a JSON report into report/cap
+ * (may be NULL; *needed gets the size). */
+GFFT_API gfft_status gfft_autotune(int32_t precision, int64_t n, int64_t count, int32_t iters, char* report,
+                                   size_t cap, size_t* needed);
+
+/* ImportWisdomFromString / ImportWisdom / ExportWisdom / ClearWisdom /
+ * WisdomLen (wisdom.go:13-82).  Lines are size:precision:features:algorithm:ts;
+ * a malformed line fails the whole import with GFFT_ERR_WISDOM and changes
+ * nothing.  Unlike the reference (plan.go:832), imported entries steer
+ * every later plan creation. */
+GFFT_API gfft_status gfft_wisdom_import_string(const char* text);
+GFFT_API gfft_status gfft_wisdom_export_string(char* buf, size_t cap, size_t* needed);
+GFFT_API gfft_status gfft_wisdom_import_file(const char* path);
+GFFT_API gfft_status gfft_wisdom_export_file(const char* path);
+GFFT_API void gfft_wisdom_clear(void);
+GFFT_API int64_t gfft_wisdom_len(void);
+
 /* ---- device-resident execution (gpu.PlanImpl, gpu/backend.go:44-51) ---- */
 
 /* Plan.Forward / Inverse (plan.go:332,382): one transform; dst may equal src. */

@@ -121,7 +121,7 @@ def test_known_answers_on_gpu(case):
     assert np.max(np.abs(y.astype(np.complex128) - want)) <= case["tol"]
 
 
-@pytest.mark.parametrize("n", [65536 // 4, 1024])
+@pytest.mark.parametrize("n", [65536, 16384, 1024])
 def test_impulse_to_ones_c128(n):
     # precision_test.go:318-405: impulse -> all ones within 1e-11, round trip 1e-10.
     x = np.zeros(n, np.complex128)
@@ -177,3 +177,94 @@ def test_strided_matches_contiguous(n, stride):
     assert rel_l2(got, ref) <= tol_c2c(n, False)
     with algofft.NewPlan(n) as p, pytest.raises(algofft.ErrInvalidStride):
         p.ForwardStrided(dst, src, 0)
+
+
+# Two-pass (four-step, L2-resident) schedule for large N.
+LARGE_C64 = [2 ** k for k in range(15, 25)]
+LARGE_C128 = [2 ** k for k in range(14, 23)]
+
+
+def _count_for(n, cap_elems=1 << 22):
+    return max(1, min(5, cap_elems // n))
+
+
+@pytest.mark.parametrize("n", LARGE_C64)
+def test_forward_inverse_c64_large(n):
+    count = _count_for(n)
+    x = seeded_complex(n * count, seed=n % 9973)
+    with algofft.NewPlan(n) as p:
+        assert "twopass" in p.Algorithm()
+        y = _run(p, x, count)
+        back = _run(p, y, count, inverse=True)
+    ref = O.batch(x[: n * min(count, 2)].astype(np.complex128), n)
+    assert rel_l2(y[: ref.size], ref) <= tol_c2c(n, False)
+    assert rel_l2(back, x) <= 2 * tol_c2c(n, False)
+
+
+@pytest.mark.parametrize("n", LARGE_C128)
+def test_forward_inverse_c128_large(n):
+    count = _count_for(n, 1 << 21)
+    x = seeded_complex(n * count, seed=n % 9973, dtype=np.complex128)
+    with algofft.NewPlan64(n) as p:
+        y = _run(p, x, count)
+        back = _run(p, y, count, inverse=True)
+    ref = O.batch(x[: n * min(count, 2)], n)
+    assert rel_l2(y[: ref.size], ref) <= tol_c2c(n, True)
+    assert rel_l2(back, x) <= 2 * tol_c2c(n, True)
+
+
+@pytest.mark.parametrize("n", [2 ** 15, 2 ** 20])
+def test_large_in_place_and_many_groups(n):
+    # enough transforms to cycle the scratch slots several times
+    count = max(3, (1 << 24) // n) + 1
+    x = seeded_complex(n * count, seed=77)
+    with algofft.NewPlan(n) as p:
+        a = _run(p, x, count)
+        b = _run(p, x, count, inplace=True)
+    assert np.array_equal(a, b)
+    idx = [0, count // 2, count - 1]
+    ref = O.batch(np.concatenate([x[i * n:(i + 1) * n] for i in idx]).astype(np.complex128), n)
+    got = np.concatenate([a[i * n:(i + 1) * n] for i in idx])
+    assert rel_l2(got, ref) <= tol_c2c(n, False)
+
+
+@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 20])
+def test_every_variant_matches_oracle(n):
+    count = max(2, (1 << 20) // n)
+    x = seeded_complex(n * count, seed=3 + n % 101)
+    ref = O.batch(x[: 2 * n].astype(np.complex128), n)
+    toks = algofft.Variants(n)
+    assert toks
+    for tok in toks:
+        with algofft.Plan(n, variant=tok) as p:
+            assert p.Algorithm() == tok
+            y = _run(p, x, count)
+            back = _run(p, y, count, inverse=True)
+            p.Check()
+        assert rel_l2(y[: 2 * n], ref) <= tol_c2c(n, False), tok
+        assert rel_l2(back, x) <= 2 * tol_c2c(n, False), tok
+
+
+def test_autotune_feeds_plan_creation():
+    algofft.ClearWisdom()
+    try:
+        rep = algofft.Autotune(4096, count=2048, iters=3)
+        assert rep["best"] in algofft.Variants(4096)
+        assert set(rep["variants"]) == set(algofft.Variants(4096))
+        with algofft.NewPlan(4096) as p:
+            assert p.Algorithm() == rep["best"]
+        # PlannerMeasure tunes on first use of a length (measure.go:89-141)
+        opts = algofft.PlanOptions(Planner=algofft.PlannerMeasure)
+        with algofft.NewPlanWithOptions(2048, opts) as p:
+            assert algofft.WisdomLen() == 2
+            assert p.Algorithm() in algofft.Variants(2048)
+    finally:
+        algofft.ClearWisdom()
+
+
+def test_forced_strategy_classes():
+    n = 8192
+    with algofft.NewPlanWithOptions(n, algofft.PlanOptions(Strategy=algofft.KernelSixStep)) as p:
+        assert "-tp-" in p.Algorithm()
+    with algofft.NewPlanWithOptions(n, algofft.PlanOptions(Strategy=algofft.KernelStockham)) as p:
+        assert "-p2-" in p.Algorithm()
