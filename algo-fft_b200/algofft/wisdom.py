@@ -53,4 +53,8 @@ def Variants(n: int, precision: int = 0) -> list[str]:
 def Autotune(n: int, precision: int = 0, count: int = 0, iters: int = 10) -> dict:
     """Times every variant on the device, records the fastest as wisdom and
     returns {"variants": {token: median ms}, "best": token, ...}."""
-    return json.loads(_read_string(lib().gfft_autotune, precision, n, count, iters))
+    cap = 1 << 16  # one call: a second call would re-run the measurement
+    buf = ctypes.create_string_buffer(cap)
+    need = ctypes.c_size_t(0)
+    check(lib().gfft_autotune(precision, n, count, iters, buf, cap, ctypes.byref(need)))
+    return json.loads(buf.value.decode())

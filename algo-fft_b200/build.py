@@ -25,7 +25,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-         "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE]
+         "-I", CSRC, "-I", INCLUDE]
 
 
 def _headers():

@@ -266,20 +266,33 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
     if (wisdom_lookup(n, prec, &tok) && core_init_variant(c, prec, n, device, tok) == GFFT_OK) return GFFT_OK;
     clear_error();
   }
-  if (pow2 && n <= max_single && !want_twopass) return init_pow2(c, default_ept(prec, n));
-  if (pow2 && !want_single) {
+  const bool want_bluestein = strategy == GFFT_KERNEL_BLUESTEIN;
+  if (pow2 && n <= max_single && !want_twopass && !want_bluestein) return init_pow2(c, default_ept(prec, n));
+  if (pow2 && !want_single && strategy != GFFT_KERNEL_BLUESTEIN) {
     const TwoPassKernel* f = find_twopass(prec, n, -1, prec == kC64 ? 8192 : 4096, prec == kC64 ? 16 : 8);
     const TwoPassKernel* i = find_twopass(prec, n, +1, prec == kC64 ? 8192 : 4096, prec == kC64 ? 16 : 8);
     if (f && i) return init_twopass(c, f, i);
   }
-  if (pow2 && n <= max_single) return init_pow2(c, default_ept(prec, n));
-  if (pow2) {
+  if (pow2 && n <= max_single && strategy != GFFT_KERNEL_BLUESTEIN) return init_pow2(c, default_ept(prec, n));
+  if (pow2 && strategy != GFFT_KERNEL_BLUESTEIN) {
     const TwoPassKernel* f = find_twopass(prec, n, -1);
     const TwoPassKernel* i = find_twopass(prec, n, +1);
     if (f && i) return init_twopass(c, f, i);
   }
-  set_error("length " + std::to_string(n) + " has no GPU schedule yet");
-  return GFFT_ERR_NOT_IMPLEMENTED;
+  // 7-smooth lengths run the runtime-radix Stockham (one CTA per transform
+  // when it fits, else two passes); everything else, or a forced
+  // KernelBluestein, goes through Bluestein (planner.go:50-55).
+  if (strategy != GFFT_KERNEL_BLUESTEIN && is_smooth7(n)) {
+    gfft_status s = init_generic(c);
+    if (s == GFFT_OK) return s;
+    core_free(c);
+    s = init_gen_twopass(c);
+    if (s == GFFT_OK) return s;
+    core_free(c);
+  }
+  if (n >= 2 && n <= (int64_t(1) << 26)) return init_bluestein(c);
+  set_error("length " + std::to_string(n) + " has no GPU schedule");
+  return GFFT_ERR_INVALID_LENGTH;
 }
 
 unsigned core_device_status(const PlanCore* c) {
@@ -294,6 +307,12 @@ void core_free(PlanCore* c) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
+  if (c->sub) {
+    core_free(c->sub);
+    delete c->sub;
+    c->sub = nullptr;
+  }
+  c->algo = Algo::Trivial;
 }
 
 static gfft_status exec_twopass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
@@ -354,6 +373,10 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
     }
     case Algo::TwoPass:
       return exec_twopass(c, dir, dst, src, count, idist, odist, st);
+    case Algo::Generic:
+    case Algo::GenTwoPass:
+    case Algo::Bluestein:
+      return exec_runtime_plan(c, dir, dst, src, count, idist, odist, st);
     case Algo::Pow2Smem: {
       const Pow2Kernel* k = c->k[dir < 0 ? 0 : 1];
       const double scale = dir < 0 ? 1.0 : 1.0 / double(c->n);

@@ -1,0 +1,178 @@
+// Runtime-schedule Stockham for any 7-smooth length (K3).
+//
+// N = product of radices from {2, 3, 4, 5, 7, 8, 16}, chosen on the host;
+// every stage is Stockham's self-sorting step (see gfft_pow2.cuh) with a
+// runtime radix dispatched to the in-register DFT codelets.  A transform's
+// data sit in shared memory (padded one element every 32) for all stages;
+// T threads own it, each thread holding up to QM butterflies of a stage in
+// registers so a stage can read all its inputs before any thread writes.
+//
+// Replaces the reference's 2/3/4/5 mixed-radix recursion
+// (internal/fft/mixedradix.go:45-420) and extends it with radix 7, which the
+// reference sends to Bluestein (internal/math/factor.go:30-43).
+#pragma once
+#include "gfft_math.cuh"
+
+namespace gfft {
+
+struct GenSched {
+  int n;          // transform length
+  int nst;        // number of stages
+  int T;          // threads per transform
+  int B;          // transforms per CTA
+  int stride;     // shared-memory elements reserved per transform
+  int radix[20];  // radix of stage s
+  int p[20];      // product of the radices before stage s
+};
+
+__device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
+
+// Butterflies a thread may hold in one stage of radix R (R*QM <= 32).
+template <int R>
+struct GenQ {
+  static constexpr int QM = R == 2 ? 16 : R == 3 ? 10 : R == 4 ? 8 : R == 5 ? 6 : R == 7 ? 4 : R == 8 ? 4 : 2;
+};
+
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void gen_stage(C* x, int n, int p, int T, int t, const C* __restrict__ tw) {
+  constexpr int QM = GenQ<R>::QM;
+  const int nb = n / R;
+  C v[QM][R];
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    const int i = t + q * T;
+    if (i < nb) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q][r] = x[gpad(i + r * nb)];
+    }
+  }
+  __syncthreads();
+  const int step = n / (p * R);
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    const int i = t + q * T;
+    if (i < nb) {
+      const int k = i % p;
+      if (p > 1) apply_twiddles<R, DIR>(v[q], __ldg(tw + k * step));
+      dft<R, DIR>(v[q]);
+      const int j = (i - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[gpad(j + r * p)] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Runs all stages on x (shared memory, padded layout) for one direction.
+template <int DIR, typename C>
+__device__ __forceinline__ void gen_fft(C* x, const GenSched& s, int t, const C* __restrict__ tw) {
+  for (int st = 0; st < s.nst; ++st) {
+    const int p = s.p[st];
+    switch (s.radix[st]) {
+      case 2: gen_stage<2, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 3: gen_stage<3, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 4: gen_stage<4, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 5: gen_stage<5, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 7: gen_stage<7, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 8: gen_stage<8, DIR>(x, s.n, p, s.T, t, tw); break;
+      default: gen_stage<16, DIR>(x, s.n, p, s.T, t, tw); break;
+    }
+  }
+}
+
+// Batched C2C with a runtime schedule: B transforms per CTA, T threads each.
+// Every thread of the CTA reaches every barrier (idle slots included).
+template <typename C, int DIR>
+__global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t count, int64_t idist,
+                                                  int64_t odist, const C* __restrict__ tw, GenSched s,
+                                                  typename RealOf<C>::type scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int slot = threadIdx.x / s.T, t = threadIdx.x % s.T;
+  C* x = reinterpret_cast<C*>(smem_raw) + slot * s.stride;
+  const int64_t b = int64_t(blockIdx.x) * s.B + slot;
+  const bool valid = slot < s.B && b < count;
+  const C* in = src + (valid ? b * idist : 0);
+  if (slot < s.B)
+    for (int e = t; e < s.n; e += s.T) x[gpad(e)] = valid ? ld_stream(in + e) : C{0, 0};
+  __syncthreads();
+  gen_fft<DIR>(x, s, slot < s.B ? t : s.T, tw);
+  if (valid) {
+    C* out = dst + b * odist;
+    for (int e = t; e < s.n; e += s.T) {
+      C y = x[gpad(e)];
+      if constexpr (DIR > 0) y = cscale(y, scale);
+      st_stream(out + e, y);
+    }
+  }
+}
+
+}  // namespace gfft
+
+namespace gfft {
+
+enum { GEN_PASS1 = 0, GEN_PASS2 = 1 };
+
+// One pass of the runtime two-pass (four-step) transform for 7-smooth
+// N = N1 * N2 (index maps as in gfft_twopass.cuh).  A CTA owns NC = s.B
+// adjacent columns of one transform, one column per slot of T threads,
+// stored column-major in shared memory with an odd per-column stride.
+//   GEN_PASS1: column n2 of x viewed as N1 x N2 (L = N1, row pitch N2),
+//              times W_N^{n2*k1}, stored as row n2 of the scratch (N2 x N1).
+//   GEN_PASS2: column k1 of the scratch (L = N2, row pitch N1), stored as
+//              column k1 of the output viewed as N2 x N1.
+// `ncols` is the row pitch of the input view (N2 in pass 1, N1 in pass 2);
+// a last partial tile masks its missing columns.
+// Loads and stores walk the tile in the order that keeps NC (pass-1 load,
+// pass-2 load and store) or L (pass-1 store) elements contiguous in HBM.
+template <typename C, int DIR, int MODE>
+__global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t count, int64_t in_dist,
+                                                   int64_t out_dist, int64_t ncols, const C* __restrict__ tw,
+                                                   GenSched s, BigTwiddle bt, typename RealOf<C>::type scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* base = reinterpret_cast<C*>(smem_raw);
+  const int L = s.n, NC = s.B;
+  const int64_t tiles = (ncols + NC - 1) / NC;
+  const int64_t b = int64_t(blockIdx.x) / tiles;
+  const int64_t col0 = (int64_t(blockIdx.x) % tiles) * NC;
+  const bool valid = b < count;
+  const C* in = src + (valid ? b * in_dist : 0);
+  C* out = dst + (valid ? b * out_dist : 0);
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int e = tid; e < L * NC; e += nthr) {
+    const int row = e / NC, c = e % NC;
+    C v = C{0, 0};
+    if (valid && col0 + c < ncols) {
+      const C* p = in + int64_t(row) * ncols + col0 + c;
+      v = MODE == GEN_PASS1 ? ld_stream(p) : __ldcg(p);
+    }
+    base[c * s.stride + gpad(row)] = v;
+  }
+  __syncthreads();
+  const int slot = tid / s.T, t = tid % s.T;
+  gen_fft<DIR>(base + (slot < NC ? slot : 0) * s.stride, s, slot < NC ? t : s.T, tw);
+  if (!valid) return;
+  if constexpr (MODE == GEN_PASS1) {
+    const C* lo = static_cast<const C*>(bt.lo);
+    const C* hi = static_cast<const C*>(bt.hi);
+    const int64_t mask = (int64_t(1) << bt.shift) - 1;
+    for (int e = tid; e < L * NC; e += nthr) {
+      const int c = e / L, k1 = e % L;
+      const int64_t n2 = col0 + c;
+      if (n2 >= ncols) continue;
+      const int64_t m = n2 * k1;
+      C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
+      if constexpr (DIR > 0) w.y = -w.y;
+      __stcg(out + n2 * L + k1, cmul(base[c * s.stride + gpad(k1)], w));
+    }
+  } else {
+    for (int e = tid; e < L * NC; e += nthr) {
+      const int k2 = e / NC, c = e % NC;
+      if (col0 + c >= ncols) continue;
+      C v = base[c * s.stride + gpad(k2)];
+      if constexpr (DIR > 0) v = cscale(v, scale);
+      st_stream(out + int64_t(k2) * ncols + col0 + c, v);
+    }
+  }
+}
+
+}  // namespace gfft

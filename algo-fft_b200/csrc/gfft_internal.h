@@ -6,6 +6,7 @@
 #include <vector>
 #include "../../include/gfft.h"
 #include "gfft_registry.h"
+#include "gfft_generic.cuh"
 
 namespace gfft {
 
@@ -20,7 +21,7 @@ gfft_status cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::gfft::cuda_status(e_, #call); \
   } while (0)
 
-enum class Algo { Trivial, Pow2Smem, TwoPass };
+enum class Algo { Trivial, Pow2Smem, TwoPass, Generic, GenTwoPass, Bluestein };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
 // FP64 and rounded to the element type (internal/math/twiddle.go:8-21).
@@ -43,7 +44,22 @@ struct PlanCore {
   int bt_shift = 0;
   int group = 1, slots = 2, resident = 1;
   unsigned* status = nullptr;  // device word: nonzero once a bounded wait expired
+  // runtime-schedule (7-smooth) plans
+  GenSched gs{}, gs1{}, gs2{};
+  int64_t gn1 = 0, gn2 = 0;
+  // Bluestein: chirps and filters per direction, sub-plan of length bm
+  PlanCore* sub = nullptr;
+  int64_t bm = 0;
+  void* bs_w[2] = {nullptr, nullptr};
+  void* bs_f[2] = {nullptr, nullptr};
 };
+
+bool is_smooth7(int64_t n);
+gfft_status init_generic(PlanCore* c);
+gfft_status init_gen_twopass(PlanCore* c);
+gfft_status init_bluestein(PlanCore* c);
+gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
+                              int64_t odist, cudaStream_t st);
 
 // Fills dst[j] = W_n^{(j*step) mod n} for j < count (FP64, rounded).
 gfft_status fill_twiddles(int prec, void* dst, int64_t n, int64_t count, int64_t step, cudaStream_t st);

@@ -51,17 +51,44 @@ template <int R, int M, int DIR, typename C> __device__ __forceinline__ C twc(C 
   }
 }
 
-template <int R> constexpr double cos_r(int m) {
+template <int R> __host__ __device__ constexpr double cos_r(int m) {
   return R == 3 ? kCos3[m] : R == 5 ? kCos5[m] : kCos7[m];
 }
-template <int R> constexpr double sin_r(int m) {
+template <int R> __host__ __device__ constexpr double sin_r(int m) {
   return R == 3 ? kSin3[m] : R == 5 ? kSin5[m] : kSin7[m];
 }
 
 // Odd prime radix (3, 5, 7): pairs s_j = v_j + v_{R-j}, d_j = v_j - v_{R-j};
-// X_k = v0 + Σ cos(2πjk/R) s_j  ±  DIR·i Σ sin(2πjk/R) d_j.
+// X_k = v0 + sum_j cos(2*pi*j*k/R) s_j  +-  DIR*i sum_j sin(2*pi*j*k/R) d_j.
+// The (j, k) loops are template recursions so every cosine/sine is a
+// compile-time constant folded into the arithmetic.
+template <int R, int K, int J, typename C>
+__device__ __forceinline__ void odd_accum(C& a, C& b, const C* s, const C* d) {
+  if constexpr (J <= (R - 1) / 2) {
+    using Re = typename RealOf<C>::type;
+    constexpr double c = cos_r<R>((J * K) % R);
+    constexpr double sn = sin_r<R>((J * K) % R);
+    a.x += Re(c) * s[J].x;
+    a.y += Re(c) * s[J].y;
+    b.x += Re(sn) * d[J].x;
+    b.y += Re(sn) * d[J].y;
+    odd_accum<R, K, J + 1>(a, b, s, d);
+  }
+}
+
+template <int R, int K, int DIR, typename C>
+__device__ __forceinline__ void odd_out(C* v, const C* s, const C* d, C x0) {
+  if constexpr (K <= (R - 1) / 2) {
+    C a = x0, b = C{0, 0};
+    odd_accum<R, K, 1>(a, b, s, d);
+    const C ib = mul_di<DIR>(b);
+    v[K] = cadd(a, ib);
+    v[R - K] = csub(a, ib);
+    odd_out<R, K + 1, DIR>(v, s, d, x0);
+  }
+}
+
 template <int R, int DIR, typename C> __device__ __forceinline__ void dft_odd(C* v) {
-  using Re = typename RealOf<C>::type;
   constexpr int H = (R - 1) / 2;
   C s[H + 1], d[H + 1];
 #pragma unroll
@@ -69,26 +96,11 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft_odd(C*
     s[j] = cadd(v[j], v[R - j]);
     d[j] = csub(v[j], v[R - j]);
   }
-  C x0 = v[0];
+  const C x0 = v[0];
   C sum = x0;
 #pragma unroll
   for (int j = 1; j <= H; ++j) sum = cadd(sum, s[j]);
-#pragma unroll
-  for (int k = 1; k <= H; ++k) {
-    C a = x0, b = C{0, 0};
-#pragma unroll
-    for (int j = 1; j <= H; ++j) {
-      const Re c = Re(cos_r<R>((j * k) % R));
-      const Re sn = Re(sin_r<R>((j * k) % R));
-      a.x += c * s[j].x;
-      a.y += c * s[j].y;
-      b.x += sn * d[j].x;
-      b.y += sn * d[j].y;
-    }
-    C ib = mul_di<DIR>(b);
-    v[k] = cadd(a, ib);
-    v[R - k] = csub(a, ib);
-  }
+  odd_out<R, 1, DIR>(v, s, d, x0);
   v[0] = sum;
 }
 
@@ -148,19 +160,55 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) 
 }
 
 // v[r] *= w^r (r = 1..RS-1) where w = tw[m] (conjugated for the inverse).
-// Powers are built as w^r = w^{floor(r/2)} * w^{ceil(r/2)}, a product tree
-// of depth ceil(log2 r), so each power carries a few ulp at most.
+// Up to RS = 8 the powers come from a product tree w^r = w^{r/2} w^{r-r/2};
+// beyond, w^r = w^{r mod 8} * (w^8)^{r/8} from the two short tables
+// {w^0..w^7} and {w^0, w^8, w^16, w^24}, which keeps ten powers live
+// instead of RS.  Tree depth, and so the rounding error, stays at a few ulp.
 template <int RS, int DIR, typename C>
 __device__ __forceinline__ void apply_twiddles(C* v, C w1) {
   if constexpr (RS > 1) {
     if constexpr (DIR > 0) w1.y = -w1.y;
-    C w[RS];
-    w[1] = w1;
+    if constexpr (RS <= 8) {
+      C w[RS];
+      w[1] = w1;
 #pragma unroll
-    for (int r = 2; r < RS; ++r) w[r] = cmul(w[r / 2], w[r - r / 2]);
+      for (int r = 2; r < RS; ++r) w[r] = cmul(w[r / 2], w[r - r / 2]);
 #pragma unroll
-    for (int r = 1; r < RS; ++r) v[r] = cmul(v[r], w[r]);
+      for (int r = 1; r < RS; ++r) v[r] = cmul(v[r], w[r]);
+    } else {
+      C lo[8], hi[RS / 8];
+      lo[1] = w1;
+#pragma unroll
+      for (int r = 2; r < 8; ++r) lo[r] = cmul(lo[r / 2], lo[r - r / 2]);
+      hi[1] = cmul(lo[4], lo[4]);
+#pragma unroll
+      for (int h = 2; h < RS / 8; ++h) hi[h] = cmul(hi[h / 2], hi[h - h / 2]);
+#pragma unroll
+      for (int r = 1; r < RS; ++r) {
+        const int a = r % 8, b = r / 8;
+        if (b == 0) v[r] = cmul(v[r], lo[a]);
+        else if (a == 0) v[r] = cmul(v[r], hi[b]);
+        else v[r] = cmul(v[r], cmul(lo[a], hi[b]));
+      }
+    }
   }
+}
+
+// W_N^m for m < N from two short tables: m = a * 2^shift + b,
+// W_N^m = hi[a] * lo[b] (one extra rounding of a complex product).
+struct BigTwiddle {
+  const void* lo;  // W_N^j, j < 2^shift
+  const void* hi;  // W_N^(j << shift), j < N >> shift
+  int shift;
+};
+
+template <typename C, int DIR>
+__device__ __forceinline__ C big_twiddle(const BigTwiddle& bt, int64_t m) {
+  const C* lo = static_cast<const C*>(bt.lo);
+  const C* hi = static_cast<const C*>(bt.hi);
+  C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & ((int64_t(1) << bt.shift) - 1))));
+  if constexpr (DIR > 0) w.y = -w.y;
+  return w;
 }
 
 // Streaming global accesses: the batch is touched exactly once.

@@ -1,0 +1,398 @@
+// Runtime-schedule plans: 7-smooth lengths (single CTA or two passes) and
+// Bluestein for every other length.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <vector>
+#include "gfft_generic.cuh"
+#include "gfft_internal.h"
+
+namespace gfft {
+
+// ------------------------------------------------------------------ schedules
+
+static bool smooth7(int64_t n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+bool is_smooth7(int64_t n) { return smooth7(n); }
+
+static int qm_of(int r) { return r == 2 ? 16 : r == 3 ? 10 : r == 4 ? 8 : r == 5 ? 6 : r == 7 ? 4 : r == 8 ? 4 : 2; }
+
+// Radix order: 16s, then the rest of the twos (8, 4, 2), then 7s, 5s, 3s.
+static bool make_sched(int64_t n, GenSched* s) {
+  *s = GenSched{};
+  if (n < 2 || n > (int64_t(1) << 30) || !smooth7(n)) return false;
+  std::vector<int> rad;
+  int64_t m = n;
+  int e2 = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++e2;
+  }
+  while (e2 >= 4) {
+    rad.push_back(16);
+    e2 -= 4;
+  }
+  if (e2 == 3) rad.push_back(8);
+  if (e2 == 2) rad.push_back(4);
+  if (e2 == 1) rad.push_back(2);
+  for (int p : {7, 5, 3})
+    while (m % p == 0) {
+      rad.push_back(p);
+      m /= p;
+    }
+  if (int(rad.size()) > 20) return false;
+  s->n = int(n);
+  s->nst = int(rad.size());
+  int64_t prod = 1, T = 1;
+  for (int i = 0; i < s->nst; ++i) {
+    s->radix[i] = rad[i];
+    s->p[i] = int(prod);
+    prod *= rad[i];
+    T = std::max<int64_t>(T, (n / rad[i] + qm_of(rad[i]) - 1) / qm_of(rad[i]));
+  }
+  if (T > 32) T = (T + 31) / 32 * 32;
+  if (T > 1024) return false;
+  s->T = int(T);
+  int stride = int(n - 1 + ((n - 1) >> 5) + 1);
+  if (stride % 2 == 0) ++stride;
+  s->stride = stride;
+  s->B = 1;
+  return true;
+}
+
+static const int kSmemBudget = 200 * 1024;
+
+// --------------------------------------------------------------- launchers
+
+template <typename C>
+static cudaError_t launch_generic(const PlanCore* c, int dir, const void* src, void* dst, int64_t count,
+                                  int64_t idist, int64_t odist, cudaStream_t st) {
+  using Re = typename RealOf<C>::type;
+  const GenSched& s = c->gs;
+  const int64_t blocks = (count + s.B - 1) / s.B;
+  const size_t smem = size_t(s.B) * s.stride * sizeof(C);
+  const Re scale = Re(1.0 / double(c->n));
+  if (dir < 0)
+    k_generic<C, -1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
+                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale);
+  else
+    k_generic<C, +1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
+                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale);
+  return cudaGetLastError();
+}
+
+template <typename C, int MODE>
+static cudaError_t launch_cols(const GenSched& s, int dir, const void* src, void* dst, int64_t count, int64_t in_dist,
+                               int64_t out_dist, int64_t ncols, const void* tw, BigTwiddle bt, double scale,
+                               cudaStream_t st) {
+  using Re = typename RealOf<C>::type;
+  const int64_t tiles = (ncols + s.B - 1) / s.B;
+  const int64_t blocks = tiles * count;
+  const size_t smem = size_t(s.B) * s.stride * sizeof(C);
+  if (blocks <= 0) return cudaSuccess;
+  if (dir < 0)
+    k_gen_cols<C, -1, MODE><<<unsigned(blocks), s.B * s.T, smem, st>>>(
+        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols,
+        static_cast<const C*>(tw), s, bt, Re(scale));
+  else
+    k_gen_cols<C, +1, MODE><<<unsigned(blocks), s.B * s.T, smem, st>>>(
+        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols,
+        static_cast<const C*>(tw), s, bt, Re(scale));
+  return cudaGetLastError();
+}
+
+static cudaError_t prepare_generic_kernels() {
+  static std::mutex mu;
+  static std::vector<int> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(mu);
+  if (std::find(done.begin(), done.end(), dev) != done.end()) return cudaSuccess;
+  const void* fns[] = {
+      reinterpret_cast<const void*>(&k_generic<float2, -1>),
+      reinterpret_cast<const void*>(&k_generic<float2, +1>),
+      reinterpret_cast<const void*>(&k_generic<double2, -1>),
+      reinterpret_cast<const void*>(&k_generic<double2, +1>),
+      reinterpret_cast<const void*>(&k_gen_cols<float2, -1, GEN_PASS1>),
+      reinterpret_cast<const void*>(&k_gen_cols<float2, +1, GEN_PASS1>),
+      reinterpret_cast<const void*>(&k_gen_cols<float2, -1, GEN_PASS2>),
+      reinterpret_cast<const void*>(&k_gen_cols<float2, +1, GEN_PASS2>),
+      reinterpret_cast<const void*>(&k_gen_cols<double2, -1, GEN_PASS1>),
+      reinterpret_cast<const void*>(&k_gen_cols<double2, +1, GEN_PASS1>),
+      reinterpret_cast<const void*>(&k_gen_cols<double2, -1, GEN_PASS2>),
+      reinterpret_cast<const void*>(&k_gen_cols<double2, +1, GEN_PASS2>),
+  };
+  for (const void* f : fns) {
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget + 16 * 1024);
+    if (e != cudaSuccess) return e;
+  }
+  done.push_back(dev);
+  return cudaSuccess;
+}
+
+// -------------------------------------------------------- 7-smooth plans
+
+// Single-CTA schedule when one transform (T <= 1024 threads, shared memory
+// within budget) fits; B transforms per CTA up to 256 threads.
+gfft_status init_generic(PlanCore* c) {
+  GenSched s;
+  const size_t es = elem_bytes(c->prec);
+  if (!make_sched(c->n, &s) || size_t(s.stride) * es > size_t(kSmemBudget)) return GFFT_ERR_NOT_IMPLEMENTED;
+  s.B = std::max(1, std::min(256 / s.T, int(kSmemBudget / (size_t(s.stride) * es))));
+  GFFT_CUDA(prepare_generic_kernels());
+  gfft_status st = make_twiddles(c->prec, c->n, &c->tw, 0);
+  if (st != GFFT_OK) return st;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->gs = s;
+  c->algo = Algo::Generic;
+  c->name = "gpu-sm100-mixed-n" + std::to_string(c->n);
+  return GFFT_OK;
+}
+
+// Column-tile schedule of length L with up to `want` columns per tile.
+static bool make_col_sched(int64_t L, size_t es, int want, GenSched* s) {
+  if (!make_sched(L, s)) return false;
+  int nc = want;
+  while (nc > 1 && (size_t(nc) * s->stride * es > size_t(kSmemBudget) || nc * s->T > 1024)) nc /= 2;
+  if (size_t(nc) * s->stride * es > size_t(kSmemBudget) || nc * s->T > 1024) return false;
+  s->B = nc;
+  return true;
+}
+
+gfft_status init_gen_twopass(PlanCore* c) {
+  const int64_t n = c->n;
+  const size_t es = elem_bytes(c->prec);
+  // N1: the 7-smooth divisor of n nearest below sqrt(n)
+  int64_t n1 = 1;
+  for (int64_t d = 1; d * d <= n; ++d)
+    if (n % d == 0 && smooth7(d)) n1 = d;
+  const int64_t n2 = n / n1;
+  if (n1 < 2) return GFFT_ERR_NOT_IMPLEMENTED;
+  const int want = c->prec == kC64 ? 16 : 8;
+  if (!make_col_sched(n1, es, want, &c->gs1) || !make_col_sched(n2, es, want, &c->gs2)) return GFFT_ERR_NOT_IMPLEMENTED;
+  GFFT_CUDA(prepare_generic_kernels());
+  int shift = 0;
+  while ((int64_t(1) << (2 * shift)) < n) ++shift;
+  const int64_t nlo = int64_t(1) << shift, nhi = (n + nlo - 1) >> shift;
+  GFFT_CUDA(cudaMalloc(&c->tw, size_t(n1 + n2 + nlo + nhi) * es));
+  char* base = static_cast<char*>(c->tw);
+  gfft_status s = fill_twiddles(c->prec, base, n1, n1, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + n1 * es, n2, n2, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + (n1 + n2) * es, n, nlo, 1, 0);
+  if (s == GFFT_OK) s = fill_twiddles(c->prec, base + (n1 + n2 + nlo) * es, n, nhi, nlo, 0);
+  if (s != GFFT_OK) return s;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->gn1 = n1;
+  c->gn2 = n2;
+  c->tw1 = base;
+  c->tw2 = base + n1 * es;
+  c->bt_lo = base + (n1 + n2) * es;
+  c->bt_hi = base + (n1 + n2 + nlo) * es;
+  c->bt_shift = shift;
+  c->algo = Algo::GenTwoPass;
+  c->name = "gpu-sm100-mixed2-" + std::to_string(n1) + "x" + std::to_string(n2);
+  return GFFT_OK;
+}
+
+static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                                    int64_t idist, int64_t odist, cudaStream_t st) {
+  const size_t es = elem_bytes(c->prec);
+  const int64_t n = c->n;
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(64) << 20) / (n * int64_t(es))));
+  void* scratch = nullptr;
+  GFFT_CUDA(cudaMallocAsync(&scratch, size_t(chunk) * size_t(n) * es, st));
+  BigTwiddle bt{c->bt_lo, c->bt_hi, c->bt_shift};
+  const double scale = 1.0 / double(n);
+  cudaError_t e = cudaSuccess;
+  for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += chunk) {
+    const int64_t m = std::min(chunk, count - b0);
+    const char* in = static_cast<const char*>(src) + size_t(b0) * size_t(idist) * es;
+    char* out = static_cast<char*>(dst) + size_t(b0) * size_t(odist) * es;
+    if (c->prec == kC64) {
+      e = launch_cols<float2, GEN_PASS1>(c->gs1, dir, in, scratch, m, idist, n, c->gn2, c->tw1, bt, 1.0, st);
+      if (e == cudaSuccess)
+        e = launch_cols<float2, GEN_PASS2>(c->gs2, dir, scratch, out, m, n, odist, c->gn1, c->tw2, bt, scale, st);
+    } else {
+      e = launch_cols<double2, GEN_PASS1>(c->gs1, dir, in, scratch, m, idist, n, c->gn2, c->tw1, bt, 1.0, st);
+      if (e == cudaSuccess)
+        e = launch_cols<double2, GEN_PASS2>(c->gs2, dir, scratch, out, m, n, odist, c->gn1, c->tw2, bt, scale, st);
+    }
+  }
+  cudaFreeAsync(scratch, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_gen_cols");
+  return GFFT_OK;
+}
+
+// ---------------------------------------------------------------- Bluestein
+
+// Chirp w_k = exp(sign * i*pi * k^2 / n) with k^2 reduced mod 2n in exact
+// integer arithmetic before the FP64 evaluation (the reference evaluates
+// float64(k*k)/n, internal/kernels/bluestein.go:20-32, which loses
+// precision as k grows).
+template <typename C>
+__global__ void k_chirp(C* w, int64_t n, int sign) {
+  using Re = typename RealOf<C>::type;
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
+    int64_t m = (k * k) % (2 * n);
+    if (m > n) m -= 2 * n;
+    double s, c;
+    sincospi(double(sign) * double(m) / double(n), &s, &c);
+    w[k] = C{Re(c), Re(s)};
+  }
+}
+
+// b_k = conj(w_k) for k < n, b_{M-k} = conj(w_k) for 0 < k < n, else 0
+// (internal/kernels/bluestein.go:39-58).
+template <typename C>
+__global__ void k_bs_filter_src(C* b, const C* w, int64_t n, int64_t M) {
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < M; j += int64_t(gridDim.x) * blockDim.x) {
+    C v{0, 0};
+    if (j < n) v = cconj(w[j]);
+    else if (M - j < n) v = cconj(w[M - j]);
+    b[j] = v;
+  }
+}
+
+// work[b][m] = m < n ? x[b][m] * w[m] : 0     (plan_bluestein.go:8-16)
+template <typename C>
+__global__ void k_bs_pre(C* work, const C* x, const C* w, int64_t n, int64_t M, int64_t count, int64_t idist) {
+  const int64_t total = count * M;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e / M, m = e - b * M;
+    work[e] = m < n ? cmul(ld_stream(x + b * idist + m), __ldg(w + m)) : C{0, 0};
+  }
+}
+
+template <typename C>
+__global__ void k_bs_mul(C* work, const C* f, int64_t M, int64_t count) {
+  const int64_t total = count * M;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x)
+    work[e] = cmul(work[e], __ldg(f + e % M));
+}
+
+// y[b][k] = work[b][k] * w[k] * scale          (plan_bluestein.go:18-58)
+template <typename C>
+__global__ void k_bs_post(C* y, const C* work, const C* w, int64_t n, int64_t M, int64_t count, int64_t odist,
+                          typename RealOf<C>::type scale) {
+  const int64_t total = count * n;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = e / n, k = e - b * n;
+    st_stream(y + b * odist + k, cscale(cmul(work[b * M + k], __ldg(w + k)), scale));
+  }
+}
+
+static unsigned grid_for(int64_t total) { return unsigned(std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 32))); }
+
+gfft_status init_bluestein(PlanCore* c) {
+  const int64_t n = c->n;
+  int64_t M = 1;
+  while (M < 2 * n - 1) M <<= 1;  // plan.go:865 NextPowerOfTwo(2n-1)
+  const size_t es = elem_bytes(c->prec);
+  c->sub = new PlanCore;
+  gfft_status s = core_init(c->sub, c->prec, M, c->device);
+  if (s != GFFT_OK) return s;
+  // [chirp fwd | chirp inv | filter fwd | filter inv]
+  GFFT_CUDA(cudaMalloc(&c->tw, size_t(2 * n + 2 * M) * es));
+  char* base = static_cast<char*>(c->tw);
+  void* wf = base;
+  void* wi = base + n * es;
+  void* ff = base + 2 * n * es;
+  void* fi = base + (2 * n + M) * es;
+  const unsigned g = grid_for(std::max(n, M));
+  if (c->prec == kC64) {
+    k_chirp<float2><<<g, 256>>>(static_cast<float2*>(wf), n, -1);
+    k_chirp<float2><<<g, 256>>>(static_cast<float2*>(wi), n, +1);
+    k_bs_filter_src<float2><<<g, 256>>>(static_cast<float2*>(ff), static_cast<float2*>(wf), n, M);
+    k_bs_filter_src<float2><<<g, 256>>>(static_cast<float2*>(fi), static_cast<float2*>(wi), n, M);
+  } else {
+    k_chirp<double2><<<g, 256>>>(static_cast<double2*>(wf), n, -1);
+    k_chirp<double2><<<g, 256>>>(static_cast<double2*>(wi), n, +1);
+    k_bs_filter_src<double2><<<g, 256>>>(static_cast<double2*>(ff), static_cast<double2*>(wf), n, M);
+    k_bs_filter_src<double2><<<g, 256>>>(static_cast<double2*>(fi), static_cast<double2*>(wi), n, M);
+  }
+  GFFT_CUDA(cudaGetLastError());
+  // filters: forward FFT_M of b (the reference's ditForward, bluestein.go:55)
+  s = core_exec(c->sub, -1, ff, ff, 1, M, M, 0);
+  if (s == GFFT_OK) s = core_exec(c->sub, -1, fi, fi, 1, M, M, 0);
+  if (s != GFFT_OK) return s;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->bm = M;
+  c->bs_w[0] = wf;
+  c->bs_w[1] = wi;
+  c->bs_f[0] = ff;
+  c->bs_f[1] = fi;
+  c->algo = Algo::Bluestein;
+  c->name = "gpu-sm100-bluestein-n" + std::to_string(n) + "-m" + std::to_string(M) + "+" + c->sub->name;
+  return GFFT_OK;
+}
+
+static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                                  int64_t idist, int64_t odist, cudaStream_t st) {
+  const size_t es = elem_bytes(c->prec);
+  const int64_t n = c->n, M = c->bm;
+  const int d = dir < 0 ? 0 : 1;
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
+  void* work = nullptr;
+  GFFT_CUDA(cudaMallocAsync(&work, size_t(chunk) * size_t(M) * es, st));
+  gfft_status s = GFFT_OK;
+  cudaError_t e = cudaSuccess;
+  const double scale = dir < 0 ? 1.0 : 1.0 / double(n);
+  for (int64_t b0 = 0; b0 < count && s == GFFT_OK && e == cudaSuccess; b0 += chunk) {
+    const int64_t m = std::min(chunk, count - b0);
+    const char* in = static_cast<const char*>(src) + size_t(b0) * size_t(idist) * es;
+    char* out = static_cast<char*>(dst) + size_t(b0) * size_t(odist) * es;
+    if (c->prec == kC64) {
+      k_bs_pre<float2><<<grid_for(m * M), 256, 0, st>>>(static_cast<float2*>(work), reinterpret_cast<const float2*>(in),
+                                                         static_cast<const float2*>(c->bs_w[d]), n, M, m, idist);
+    } else {
+      k_bs_pre<double2><<<grid_for(m * M), 256, 0, st>>>(static_cast<double2*>(work), reinterpret_cast<const double2*>(in),
+                                                          static_cast<const double2*>(c->bs_w[d]), n, M, m, idist);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) break;
+    s = core_exec(c->sub, -1, work, work, m, M, M, st);
+    if (s != GFFT_OK) break;
+    if (c->prec == kC64)
+      k_bs_mul<float2><<<grid_for(m * M), 256, 0, st>>>(static_cast<float2*>(work), static_cast<const float2*>(c->bs_f[d]), M, m);
+    else
+      k_bs_mul<double2><<<grid_for(m * M), 256, 0, st>>>(static_cast<double2*>(work), static_cast<const double2*>(c->bs_f[d]), M, m);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) break;
+    s = core_exec(c->sub, +1, work, work, m, M, M, st);  // includes 1/M (bluestein.go:76)
+    if (s != GFFT_OK) break;
+    if (c->prec == kC64)
+      k_bs_post<float2><<<grid_for(m * n), 256, 0, st>>>(reinterpret_cast<float2*>(out), static_cast<const float2*>(work),
+                                                          static_cast<const float2*>(c->bs_w[d]), n, M, m, odist, float(scale));
+    else
+      k_bs_post<double2><<<grid_for(m * n), 256, 0, st>>>(reinterpret_cast<double2*>(out), static_cast<const double2*>(work),
+                                                           static_cast<const double2*>(c->bs_w[d]), n, M, m, odist, scale);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(work, st);
+  if (e != cudaSuccess) return cuda_status(e, "bluestein");
+  return s;
+}
+
+gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
+                              int64_t odist, cudaStream_t st) {
+  switch (c->algo) {
+    case Algo::Generic:
+      GFFT_CUDA(c->prec == kC64 ? launch_generic<float2>(c, dir, src, dst, count, idist, odist, st)
+                                : launch_generic<double2>(c, dir, src, dst, count, idist, odist, st));
+      return GFFT_OK;
+    case Algo::GenTwoPass:
+      return exec_gen_twopass(c, dir, dst, src, count, idist, odist, st);
+    case Algo::Bluestein:
+      return exec_bluestein(c, dir, dst, src, count, idist, odist, st);
+    default:
+      return GFFT_ERR_NOT_IMPLEMENTED;
+  }
+}
+
+}  // namespace gfft

@@ -40,10 +40,13 @@ __device__ __forceinline__ void xsync() {
   else __syncthreads();
 }
 
-template <typename C, int N, int EPT, int DIR, int P>
-__device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int t, bool valid,
-                                           const C* __restrict__ tw,
-                                           typename RealOf<C>::type scale) {
+// Stage recursion of one length-N transform owned by T threads.  The first
+// stage takes its inputs from ld(e) and the last hands its outputs to
+// st(e, value) (e = element index in natural order), so callers fuse their
+// own prologue and epilogue (global I/O, pre-/post-twiddles, real-FFT
+// repacking, Bluestein chirps) into the transform.
+template <typename C, int N, int EPT, int DIR, int P, typename LD, typename ST>
+__device__ __forceinline__ void pow2_stage(C* v, C* sh, int t, const C* __restrict__ tw, LD& ld, ST& st) {
   using S = Pow2Shape<N, EPT, sizeof(C)>;
   using SC = Sched<N, EPT>;
   constexpr int T = S::T;
@@ -57,7 +60,7 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
-      for (int r = 0; r < RS; ++r) v[q * RS + r] = valid ? ld_stream(in + (t + q * T + r * STRIDE)) : C{0, 0};
+      for (int r = 0; r < RS; ++r) v[q * RS + r] = ld(t + q * T + r * STRIDE);
   } else {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -82,16 +85,10 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
   }
 
   if constexpr (LAST) {
-    if (valid) {
 #pragma unroll
-      for (int q = 0; q < Q; ++q)
+    for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int r = 0; r < RS; ++r) {
-          C o = v[q * RS + r];
-          if constexpr (DIR > 0) o = cscale(o, scale);
-          st_stream(out + (t + q * T + r * P), o);
-        }
-    }
+      for (int r = 0; r < RS; ++r) st(t + q * T + r * P, v[q * RS + r]);
   } else {
     if constexpr (!FIRST) xsync<T>();
 #pragma unroll
@@ -111,9 +108,33 @@ __device__ __forceinline__ void pow2_stage(C* v, const C* in, C* out, C* sh, int
       }
     }
     xsync<T>();
-    pow2_stage<C, N, EPT, DIR, P * RS>(v, in, out, sh, t, valid, tw, scale);
+    pow2_stage<C, N, EPT, DIR, P * RS>(v, sh, t, tw, ld, st);
   }
 }
+
+template <typename C, int N, int EPT, int DIR, typename LD, typename ST>
+__device__ __forceinline__ void pow2_fft(C* sh, int t, const C* __restrict__ tw, LD& ld, ST& st) {
+  C v[EPT];
+  pow2_stage<C, N, EPT, DIR, 1>(v, sh, t, tw, ld, st);
+}
+
+template <typename C>
+struct GlobalLoad {
+  const C* in;
+  bool valid;
+  __device__ __forceinline__ C operator()(int e) const { return valid ? ld_stream(in + e) : C{0, 0}; }
+};
+
+template <typename C, bool SCALE>
+struct GlobalStore {
+  C* out;
+  bool valid;
+  typename RealOf<C>::type scale;
+  __device__ __forceinline__ void operator()(int e, C x) const {
+    if constexpr (SCALE) x = cscale(x, scale);
+    if (valid) st_stream(out + e, x);
+  }
+};
 
 // Batched C2C: transform b reads src[b*idist .. b*idist+N) and writes
 // dst[b*odist ..).  src may equal dst (every CTA reads its whole transform
@@ -128,10 +149,9 @@ k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const 
   const int t = threadIdx.x % S::T;
   const int64_t b = int64_t(blockIdx.x) * S::B + threadIdx.x / S::T;
   const bool valid = b < count;
-  const C* in = src + (valid ? b * idist : 0);
-  C* out = dst + (valid ? b * odist : 0);
-  C v[EPT];
-  pow2_stage<C, N, EPT, DIR, 1>(v, in, out, sh, t, valid, tw, scale);
+  GlobalLoad<C> ld{src + (valid ? b * idist : 0), valid};
+  GlobalStore<C, (DIR > 0)> st{dst + (valid ? b * odist : 0), valid, scale};
+  pow2_fft<C, N, EPT, DIR>(sh, t, tw, ld, st);
 }
 
 }  // namespace gfft

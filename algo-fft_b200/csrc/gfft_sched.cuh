@@ -9,8 +9,8 @@ namespace gfft {
 
 template <int L, int EPT>
 struct Sched {
-  static constexpr int radix_at(int P) { return (P * EPT <= L) ? EPT : L / P; }
-  static constexpr int num_stages() {
+  __host__ __device__ static constexpr int radix_at(int P) { return (P * EPT <= L) ? EPT : L / P; }
+  __host__ __device__ static constexpr int num_stages() {
     int s = 0;
     for (int p = 1; p < L; p *= radix_at(p)) ++s;
     return s;

@@ -48,21 +48,6 @@ struct ColShape {
   }
 };
 
-struct BigTwiddle {
-  const void* lo;  // W_N^j, j < 2^shift
-  const void* hi;  // W_N^(j << shift), j < N >> shift
-  int shift;
-};
-
-template <typename C, int DIR>
-__device__ __forceinline__ C big_twiddle(const BigTwiddle& bt, int64_t m) {
-  const C* lo = static_cast<const C*>(bt.lo);
-  const C* hi = static_cast<const C*>(bt.hi);
-  C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & ((int64_t(1) << bt.shift) - 1))));
-  if constexpr (DIR > 0) w.y = -w.y;
-  return w;
-}
-
 enum { LOAD_STREAM = 0, LOAD_L2 = 1 };
 enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1 };
 
@@ -74,9 +59,9 @@ __device__ __forceinline__ C gload(const C* p) {
 
 // One Stockham stage of a column tile (see pow2_stage for the algebra).
 // Element (row, c) of the tile lives at sh[phys(row, c)]; global row r of
-// column c is at in[r*istride + c].
-template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE>
-__device__ __forceinline__ void col_stage(C* v, const C* in, int64_t istride, C* out, int64_t ostride, C* sh,
+// column c is at in[r*ISTRIDE + c].
+template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE>
+__device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
                                           int t, int c, bool active, const C* __restrict__ tw,
                                           typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2) {
   using S = ColShape<L, EPT, NC, sizeof(C)>;
@@ -94,7 +79,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, int64_t istride, C*
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int r = 0; r < RS; ++r)
-          v[q * RS + r] = gload<LOADK>(in + int64_t(t + q * T + r * STRIDE) * istride + c);
+          v[q * RS + r] = gload<LOADK>(in + int64_t(t + q * T + r * STRIDE) * ISTRIDE + c);
     } else {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
@@ -119,19 +104,31 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, int64_t istride, C*
         for (int r = 0; r < RS; ++r) {
           C o = v[q * RS + r];
           if constexpr (DIR > 0) o = cscale(o, scale);
-          st_stream(out + int64_t(t + q * T + r * P) * ostride + c, o);
+          st_stream(out + int64_t(t + q * T + r * P) * OSTRIDE + c, o);
         }
     }
   } else if constexpr (LAST) {
     if constexpr (!FIRST) __syncthreads();
     if (active) {
+      // W_N^{n2*(row0 + r*P)} = b * s^r with b = W_N^{n2*row0} (one lookup per
+      // butterfly) and s = W_N^{n2*P} (one per thread); the powers of s come
+      // from a product tree, so no per-element table lookup is scattered
+      // across the warp.
+      const C s = big_twiddle<C, DIR>(bt, n2 * P);
+      C pw[RS];
+      pw[0] = C{1, 0};
+      if constexpr (RS > 1) pw[1] = s;
+#pragma unroll
+      for (int r = 2; r < RS; ++r) pw[r] = cmul(pw[r / 2], pw[r - r / 2]);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int row0 = t + q * T;
-        const int64_t m0 = n2 * row0, dm = n2 * P;
+        const C b = big_twiddle<C, DIR>(bt, n2 * row0);
 #pragma unroll
-        for (int r = 0; r < RS; ++r)
-          sh[S::phys(row0 + r * P, c)] = cmul(v[q * RS + r], big_twiddle<C, DIR>(bt, m0 + r * dm));
+        for (int r = 0; r < RS; ++r) {
+          const C w = r == 0 ? b : cmul(b, pw[r]);
+          sh[S::phys(row0 + r * P, c)] = cmul(v[q * RS + r], w);
+        }
       }
     }
     __syncthreads();
@@ -148,8 +145,8 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, int64_t istride, C*
       }
     }
     __syncthreads();
-    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE>(v, in, istride, out, ostride, sh, t, c, active, tw, scale,
-                                                       bt, n2);
+    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE>(v, in, out, sh, t, c, active, tw, scale,
+                                                                         bt, n2);
   }
 }
 
@@ -281,8 +278,8 @@ k_twopass(TwoPassParams p) {
       const int c = tid % NC1, t = tid / NC1;
       const C* in = src + (valid ? b * p.idist : 0) + col0;
       C* y = scratch + (int64_t(slot) * p.G + (b - int64_t(g) * p.G)) * TP::N;
-      col_stage<C, N1, EPT1, NC1, DIR, 1, LOAD_STREAM, OUT_SMEM_TWIDDLE>(
-          v, in, N2, nullptr, 0, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c));
+      col_stage<C, N1, EPT1, NC1, DIR, 1, LOAD_STREAM, OUT_SMEM_TWIDDLE, N2, 0>(
+          v, in, nullptr, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c));
       if (valid) {
         // transposed store: Y[col0 + cc][row], rows of N1 contiguous
         for (int e = tid; e < N1 * NC1; e += TP::TPB) {
@@ -298,9 +295,9 @@ k_twopass(TwoPassParams p) {
       const int c = tid % NC2, t = tid / NC2;
       const C* y = scratch + (int64_t(slot) * p.G + (b - int64_t(g) * p.G)) * TP::N + col0;
       C* out = dst + (valid ? b * p.odist : 0) + col0;
-      col_stage<C, N2, EPT2, NC2, DIR, 1, LOAD_L2, OUT_COLUMNS>(v, y, N1, out, N1, sh, t, c, active,
-                                                                static_cast<const C*>(p.tw2), Re(p.scale),
-                                                                p.bt, 0);
+      col_stage<C, N2, EPT2, NC2, DIR, 1, LOAD_L2, OUT_COLUMNS, N1, N1>(v, y, out, sh, t, c, active,
+                                                                        static_cast<const C*>(p.tw2), Re(p.scale),
+                                                                        p.bt, 0);
     }
     __syncthreads();
     if (tid == 0) {
