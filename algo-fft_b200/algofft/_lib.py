@@ -106,6 +106,7 @@ SIGNATURES = {
     "gfft_inverse_batch": (I32, [P, P, I64, P, I64, I64, P]),
     "gfft_forward_strided": (I32, [P, P, I64, P, I64, I64, P]),
     "gfft_inverse_strided": (I32, [P, P, I64, P, I64, I64, P]),
+    "gfft_exec_batch_noalloc": (I32, [P, I32, P, I64, P, I64, I64, P]),
     "gfft_forward_host": (I32, [P, P, I64, P, I64]),
     "gfft_inverse_host": (I32, [P, P, I64, P, I64]),
     "gfft_forward_batch_host": (I32, [P, P, I64, P, I64, I64]),

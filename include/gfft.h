@@ -160,6 +160,22 @@ GFFT_API gfft_status gfft_forward_strided(gfft_plan* plan, void* dst, int64_t ds
 GFFT_API gfft_status gfft_inverse_strided(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
                                  int64_t stride, void* stream);
 
+/* Batched transform (direction -1 forward, +1 inverse; contiguous
+ * [i*n, (i+1)*n) layout, validated like ForwardBatch) that allocates
+ * nothing.  No counterpart in the reference: it exists for callers that must
+ * not allocate while they run a transform (a real-time or callback context,
+ * a process whose GPU allocator belongs to another runtime, a service that
+ * reserves its memory up front).  It runs the plan's two-pass large-N
+ * kernel with its scratch in a fixed 64 MiB array inside the library (held
+ * on every GPU that loads the library until the process exits) instead of
+ * the stream-ordered pool, so a length-n transform needs 2*n*element_size
+ * bytes of it at most 63.5 MiB (n <= 2^21 complex64, 2^20 complex128);
+ * larger lengths, or plans on another schedule, are rejected with an error.
+ * The first call on a device looks the array up (make it before any stream
+ * capture).  All calls share the array: calls that overlap on the GPU race. */
+GFFT_API gfft_status gfft_exec_batch_noalloc(gfft_plan* plan, int32_t direction, void* dst, int64_t dst_len,
+                                             const void* src, int64_t src_len, int64_t count, void* stream);
+
 /* ---- host-slice execution (the Go-slice methods) ------------------------ */
 
 GFFT_API gfft_status gfft_forward_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len);
