@@ -111,6 +111,14 @@ SIGNATURES = {
     "gfft_inverse_host": (I32, [P, P, I64, P, I64]),
     "gfft_forward_batch_host": (I32, [P, P, I64, P, I64, I64]),
     "gfft_inverse_batch_host": (I32, [P, P, I64, P, I64, I64]),
+    "gfft_plan_real_new": (I32, [PP, I32, I64, ctypes.POINTER(PlanOptionsC)]),
+    "gfft_plan_real_close": (None, [P]),
+    "gfft_plan_real_len": (I64, [P]),
+    "gfft_plan_real_spectrum_len": (I64, [P]),
+    "gfft_real_forward": (I32, [P, I32, P, I64, P, I64, P]),
+    "gfft_real_inverse": (I32, [P, P, I64, P, I64, P]),
+    "gfft_real_forward_host": (I32, [P, I32, P, I64, P, I64]),
+    "gfft_real_inverse_host": (I32, [P, P, I64, P, I64]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

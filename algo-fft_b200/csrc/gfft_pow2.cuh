@@ -44,7 +44,9 @@ __device__ __forceinline__ void xsync() {
 // stage takes its inputs from ld(e) and the last hands its outputs to
 // st(e, value) (e = element index in natural order), so callers fuse their
 // own prologue and epilogue (global I/O, pre-/post-twiddles, real-FFT
-// repacking, Bluestein chirps) into the transform.
+// repacking, Bluestein chirps) into the transform.  A policy with
+// kShared = true reads or writes this transform's shared memory, and the
+// stage then adds the barrier that in-place reuse needs.
 template <typename C, int N, int EPT, int DIR, int P, typename LD, typename ST>
 __device__ __forceinline__ void pow2_stage(C* v, C* sh, int t, const C* __restrict__ tw, LD& ld, ST& st) {
   using S = Pow2Shape<N, EPT, sizeof(C)>;
@@ -85,12 +87,15 @@ __device__ __forceinline__ void pow2_stage(C* v, C* sh, int t, const C* __restri
   }
 
   if constexpr (LAST) {
+    // a store policy that writes back into this transform's shared memory
+    // must wait until every thread has read the last stage's inputs
+    if constexpr (ST::kShared && !(FIRST && !LD::kShared)) xsync<T>();
 #pragma unroll
     for (int q = 0; q < Q; ++q)
 #pragma unroll
       for (int r = 0; r < RS; ++r) st(t + q * T + r * P, v[q * RS + r]);
   } else {
-    if constexpr (!FIRST) xsync<T>();
+    if constexpr (!FIRST || LD::kShared) xsync<T>();
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int i = t + q * T;
@@ -120,6 +125,7 @@ __device__ __forceinline__ void pow2_fft(C* sh, int t, const C* __restrict__ tw,
 
 template <typename C>
 struct GlobalLoad {
+  static constexpr bool kShared = false;
   const C* in;
   bool valid;
   __device__ __forceinline__ C operator()(int e) const { return valid ? ld_stream(in + e) : C{0, 0}; }
@@ -127,6 +133,7 @@ struct GlobalLoad {
 
 template <typename C, bool SCALE>
 struct GlobalStore {
+  static constexpr bool kShared = false;
   C* out;
   bool valid;
   typename RealOf<C>::type scale;

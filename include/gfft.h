@@ -185,6 +185,38 @@ GFFT_API gfft_status gfft_forward_batch_host(gfft_plan* plan, void* dst, int64_t
 GFFT_API gfft_status gfft_inverse_batch_host(gfft_plan* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
                                     int64_t count);
 
+/* ---- real-input plans (PlanReal, plan_real_generic.go) -------------------- */
+
+/* Opaque PlanRealT[F, C] (plan_real_generic.go:22-36). */
+typedef struct gfft_plan_real gfft_plan_real;
+
+/* NewPlanReal32/64 / NewPlanRealTWithOptions (plan_real_constructors.go:8-43,
+ * plan_real_generic.go:48-99): n reals, n even (else GFFT_ERR_INVALID_LENGTH).
+ * precision GFFT_COMPLEX64 means float32 in / complex64 out.  opts->batch and
+ * opts->stride give the batch layout of plan_batch.go:21-42 (the stride, in
+ * elements, applies to the reals and to the bins alike). */
+GFFT_API gfft_status gfft_plan_real_new(gfft_plan_real** out, int32_t precision, int64_t n,
+                                        const gfft_plan_options* opts);
+GFFT_API void gfft_plan_real_close(gfft_plan_real* plan);
+/* Len / SpectrumLen (plan_real_generic.go:101-109): n and n/2+1. */
+GFFT_API int64_t gfft_plan_real_len(const gfft_plan_real* plan);
+GFFT_API int64_t gfft_plan_real_spectrum_len(const gfft_plan_real* plan);
+
+/* Forward (R2C, plan_real_generic.go:111), ForwardNormalized (scaling 1,
+ * x 1/n, :231) and ForwardUnitary (scaling 2, x 1/sqrt(n), :243); scaling 0 is
+ * the plain Forward.  dst: n/2+1 complex bins, src: n reals (per transform). */
+GFFT_API gfft_status gfft_real_forward(gfft_plan_real* plan, int32_t scaling, void* dst, int64_t dst_len,
+                                       const void* src, int64_t src_len, void* stream);
+/* Inverse (C2R, plan_real_generic.go:256): returns GFFT_ERR_INVALID_SPECTRUM
+ * if a DC or Nyquist bin has |imag| > 1e-4 (float32) / 1e-12 (float64)
+ * (:301-316); checking it synchronizes the stream. */
+GFFT_API gfft_status gfft_real_inverse(gfft_plan_real* plan, void* dst, int64_t dst_len, const void* src,
+                                       int64_t src_len, void* stream);
+GFFT_API gfft_status gfft_real_forward_host(gfft_plan_real* plan, int32_t scaling, void* dst, int64_t dst_len,
+                                            const void* src, int64_t src_len);
+GFFT_API gfft_status gfft_real_inverse_host(gfft_plan_real* plan, void* dst, int64_t dst_len, const void* src,
+                                            int64_t src_len);
+
 /* ---- errors -------------------------------------------------------------- */
 
 /* Text of a status code (the reference's error strings for 1..6). */
