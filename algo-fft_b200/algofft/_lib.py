@@ -119,6 +119,17 @@ SIGNATURES = {
     "gfft_real_inverse": (I32, [P, P, I64, P, I64, P]),
     "gfft_real_forward_host": (I32, [P, I32, P, I64, P, I64]),
     "gfft_real_inverse_host": (I32, [P, P, I64, P, I64]),
+    "gfft_plan_nd_new": (I32, [PP, I32, I32, ctypes.POINTER(I64), I32, ctypes.POINTER(PlanOptionsC)]),
+    "gfft_plan_nd_close": (None, [P]),
+    "gfft_plan_nd_len": (I64, [P]),
+    "gfft_plan_nd_spectrum_len": (I64, [P]),
+    "gfft_nd_forward": (I32, [P, P, I64, P, I64, P]),
+    "gfft_nd_inverse": (I32, [P, P, I64, P, I64, P]),
+    "gfft_nd_forward_full": (I32, [P, P, I64, P, I64, P]),
+    "gfft_nd_inverse_full": (I32, [P, P, I64, P, I64, P]),
+    "gfft_nd_forward_host": (I32, [P, P, I64, P, I64]),
+    "gfft_nd_inverse_host": (I32, [P, P, I64, P, I64]),
+    "gfft_exec_strided_batch": (I32, [P, I32, P, I64, P, I64, I64, I64, I64, P]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

@@ -163,6 +163,13 @@ class Plan:
         """plan_strided.go:25 (device buffers)."""
         return self._strided("gfft_inverse_strided", dst, src, stride)
 
+    def StridedBatch(self, dst, src, count: int, stride: int, dist: int, inverse: bool = False):
+        """count transforms, element j of transform b at b*dist + j*stride (device buffers)."""
+        dp, dl, dd = _ptr_len(dst)
+        sp, sl, sd = _ptr_len(src)
+        check(lib().gfft_exec_strided_batch(self._h, 1 if inverse else -1, dp, dl, sp, sl, count, stride, dist,
+                                            _stream(dst)))
+
     def _strided(self, fn, dst, src, stride):
         if dst is None or src is None:
             raise ErrNilSlice("algo-fft: nil slice")

@@ -120,14 +120,16 @@ enum { GEN_PASS1 = 0, GEN_PASS2 = 1 };
 //              times W_N^{n2*k1}, stored as row n2 of the scratch (N2 x N1).
 //   GEN_PASS2: column k1 of the scratch (L = N2, row pitch N1), stored as
 //              column k1 of the output viewed as N2 x N1.
-// `ncols` is the row pitch of the input view (N2 in pass 1, N1 in pass 2);
+// `ncols` columns (N2 in pass 1, N1 in pass 2) with rows `pitch` elements
+// apart (pitch = ncols in the four-step; larger for strided column batches);
 // a last partial tile masks its missing columns.
 // Loads and stores walk the tile in the order that keeps NC (pass-1 load,
 // pass-2 load and store) or L (pass-1 store) elements contiguous in HBM.
 template <typename C, int DIR, int MODE>
 __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t count, int64_t in_dist,
-                                                   int64_t out_dist, int64_t ncols, const C* __restrict__ tw,
-                                                   GenSched s, BigTwiddle bt, typename RealOf<C>::type scale) {
+                                                   int64_t out_dist, int64_t ncols, int64_t pitch,
+                                                   const C* __restrict__ tw, GenSched s, BigTwiddle bt,
+                                                   typename RealOf<C>::type scale) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* base = reinterpret_cast<C*>(smem_raw);
   const int L = s.n, NC = s.B;
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
     const int row = e / NC, c = e % NC;
     C v = C{0, 0};
     if (valid && col0 + c < ncols) {
-      const C* p = in + int64_t(row) * ncols + col0 + c;
+      const C* p = in + int64_t(row) * pitch + col0 + c;
       v = MODE == GEN_PASS1 ? ld_stream(p) : __ldcg(p);
     }
     base[c * s.stride + gpad(row)] = v;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
       if (col0 + c >= ncols) continue;
       C v = base[c * s.stride + gpad(k2)];
       if constexpr (DIR > 0) v = cscale(v, scale);
-      st_stream(out + int64_t(k2) * ncols + col0 + c, v);
+      st_stream(out + int64_t(k2) * pitch + col0 + c, v);
     }
   }
 }

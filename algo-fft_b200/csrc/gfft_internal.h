@@ -58,6 +58,10 @@ bool is_smooth7(int64_t n);
 gfft_status init_generic(PlanCore* c);
 gfft_status init_gen_twopass(PlanCore* c);
 gfft_status init_bluestein(PlanCore* c);
+// Column batches through the runtime column kernel (7-smooth n that fits).
+bool column_sched(int64_t n, int prec, GenSched* s);
+gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const void* src, int64_t count,
+                         int64_t dist, int64_t ncols, int64_t pitch, const void* tw_n, cudaStream_t st);
 gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
                               int64_t odist, cudaStream_t st);
 
@@ -98,3 +102,27 @@ struct gfft_plan {
   gfft::PlanCore core;
   gfft_plan_options opts{};
 };
+
+namespace gfft {
+struct RealKernel;
+}
+
+struct gfft_plan_real {
+  gfft::PlanCore child;  // half-length complex plan (plan_real_generic.go:64)
+  int prec = 0;
+  int64_t n = 0, h = 0;
+  gfft_plan_options opts{};
+  void* wt = nullptr;  // U[k], k <= h
+  const gfft::RealKernel* fused = nullptr;
+  unsigned* flag = nullptr;
+};
+
+namespace gfft {
+// Batched real transforms on device buffers: `batch` transforms, reals
+// `sr` apart and spectra `sc` apart (element units); scaling 0 none,
+// 1 x 1/n, 2 x 1/sqrt(n).
+gfft_status real_forward(gfft_plan_real* p, int scaling, void* dst, const void* src, int64_t batch, int64_t sr,
+                         int64_t sc, cudaStream_t st);
+gfft_status real_inverse(gfft_plan_real* p, void* dst, const void* src, int64_t batch, int64_t sr, int64_t sc,
+                         cudaStream_t st);
+}  // namespace gfft

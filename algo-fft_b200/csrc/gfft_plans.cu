@@ -89,7 +89,8 @@ static cudaError_t launch_generic(const PlanCore* c, int dir, const void* src, v
 template <typename C, int MODE>
 static cudaError_t launch_cols(const GenSched& s, int dir, const void* src, void* dst, int64_t count, int64_t in_dist,
                                int64_t out_dist, int64_t ncols, const void* tw, BigTwiddle bt, double scale,
-                               cudaStream_t st) {
+                               cudaStream_t st, int64_t pitch = -1) {
+  if (pitch < 0) pitch = ncols;
   using Re = typename RealOf<C>::type;
   const int64_t tiles = (ncols + s.B - 1) / s.B;
   const int64_t blocks = tiles * count;
@@ -97,11 +98,11 @@ static cudaError_t launch_cols(const GenSched& s, int dir, const void* src, void
   if (blocks <= 0) return cudaSuccess;
   if (dir < 0)
     k_gen_cols<C, -1, MODE><<<unsigned(blocks), s.B * s.T, smem, st>>>(
-        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols,
+        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols, pitch,
         static_cast<const C*>(tw), s, bt, Re(scale));
   else
     k_gen_cols<C, +1, MODE><<<unsigned(blocks), s.B * s.T, smem, st>>>(
-        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols,
+        static_cast<const C*>(src), static_cast<C*>(dst), count, in_dist, out_dist, ncols, pitch,
         static_cast<const C*>(tw), s, bt, Re(scale));
   return cudaGetLastError();
 }
@@ -225,6 +226,23 @@ static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const
     }
   }
   cudaFreeAsync(scratch, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_gen_cols");
+  return GFFT_OK;
+}
+
+// Column batch: `count` blocks `dist` apart, each holding ncols transforms of
+// length s.n laid out as columns (element j of column c at j*pitch + c).
+bool column_sched(int64_t n, int prec, GenSched* s) {
+  return make_col_sched(n, elem_bytes(prec), prec == kC64 ? 16 : 8, s) && (prepare_generic_kernels() == cudaSuccess);
+}
+
+gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const void* src, int64_t count,
+                         int64_t dist, int64_t ncols, int64_t pitch, const void* tw_n, cudaStream_t st) {
+  BigTwiddle bt{nullptr, nullptr, 0};
+  const double scale = 1.0 / double(s.n);
+  cudaError_t e = prec == kC64
+                      ? launch_cols<float2, GEN_PASS2>(s, dir, src, dst, count, dist, dist, ncols, tw_n, bt, scale, st, pitch)
+                      : launch_cols<double2, GEN_PASS2>(s, dir, src, dst, count, dist, dist, ncols, tw_n, bt, scale, st, pitch);
   if (e != cudaSuccess) return cuda_status(e, "k_gen_cols");
   return GFFT_OK;
 }

@@ -130,16 +130,6 @@ static unsigned grid1(int64_t total) { return unsigned(std::max<int64_t>(1, std:
 
 using namespace gfft;
 
-struct gfft_plan_real {
-  PlanCore child;  // half-length complex plan (plan_real_generic.go:64)
-  int prec = 0;
-  int64_t n = 0, h = 0;
-  gfft_plan_options opts{};
-  void* wt = nullptr;  // U[k], k <= h
-  const RealKernel* fused = nullptr;
-  unsigned* flag = nullptr;
-};
-
 extern "C" {
 
 gfft_status gfft_plan_real_new(gfft_plan_real** out, int32_t precision, int64_t n, const gfft_plan_options* opts) {
@@ -225,7 +215,7 @@ static gfft_status real_layout(const gfft_plan_real* p, int64_t real_len, int64_
   return GFFT_OK;
 }
 
-static gfft_status real_forward(gfft_plan_real* p, int scaling, void* dst, const void* src, int64_t batch, int64_t sr,
+gfft_status real_forward(gfft_plan_real* p, int scaling, void* dst, const void* src, int64_t batch, int64_t sr,
                                 int64_t sc, cudaStream_t st) {
   const size_t es = elem_bytes(p->prec);
   const double scale = scaling == 1 ? 1.0 / double(p->n) : scaling == 2 ? 1.0 / std::sqrt(double(p->n)) : 1.0;
@@ -257,7 +247,7 @@ static gfft_status real_forward(gfft_plan_real* p, int scaling, void* dst, const
   return s;
 }
 
-static gfft_status real_inverse(gfft_plan_real* p, void* dst, const void* src, int64_t batch, int64_t sr, int64_t sc,
+gfft_status real_inverse(gfft_plan_real* p, void* dst, const void* src, int64_t batch, int64_t sr, int64_t sc,
                                 cudaStream_t st) {
   const size_t es = elem_bytes(p->prec);
   // DC and Nyquist must be real (plan_real_generic.go:301-316)

@@ -217,6 +217,53 @@ GFFT_API gfft_status gfft_real_forward_host(gfft_plan_real* plan, int32_t scalin
 GFFT_API gfft_status gfft_real_inverse_host(gfft_plan_real* plan, void* dst, int64_t dst_len, const void* src,
                                             int64_t src_len);
 
+/* ---- N-dimensional plans ------------------------------------------------- */
+
+/* Opaque Plan2D / Plan3D / PlanND (plan_2d.go, plan_3d.go, plan_nd.go) and,
+ * with real_input = 1, PlanReal2D / PlanReal3D (plan_real_2d.go,
+ * plan_real_3d.go; any rank here). */
+typedef struct gfft_plan_nd gfft_plan_nd;
+
+/* NewPlan2D/3D/ND[WithOptions] (plan_2d.go:28, plan_3d.go:42-49,
+ * plan_nd.go:43-50), NewPlanReal2D/3D (plan_real_2d.go:43-48,
+ * plan_real_3d.go:42): row-major dims[0] x ... x dims[ndims-1], 1 <= ndims
+ * <= 8, every dim >= 1 (real: last dim even) else GFFT_ERR_INVALID_LENGTH.
+ * opts->batch / opts->stride: the batch layout of plan_batch.go:3-42. */
+GFFT_API gfft_status gfft_plan_nd_new(gfft_plan_nd** out, int32_t precision, int32_t ndims, const int64_t* dims,
+                                      int32_t real_input, const gfft_plan_options* opts);
+GFFT_API void gfft_plan_nd_close(gfft_plan_nd* plan);
+/* Len (plan_nd.go:151): product of dims.  SpectrumLen (plan_real_2d.go:121):
+ * the compact spectrum, product of dims with the last one n/2+1 (= Len for
+ * complex plans). */
+GFFT_API int64_t gfft_plan_nd_len(const gfft_plan_nd* plan);
+GFFT_API int64_t gfft_plan_nd_spectrum_len(const gfft_plan_nd* plan);
+/* Forward / Inverse (plan_nd.go:188, plan_real_2d.go:139,278): complex plans
+ * map Len -> Len elements (dst may equal src); real plans map Len reals to
+ * SpectrumLen bins and back (the inverse leaves src untouched and checks the
+ * last axis' DC/Nyquist bins like PlanReal.Inverse). */
+GFFT_API gfft_status gfft_nd_forward(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                     void* stream);
+GFFT_API gfft_status gfft_nd_inverse(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src, int64_t src_len,
+                                     void* stream);
+/* ForwardFull / InverseFull of real plans (plan_real_2d.go:231,370): the
+ * full Len-bin spectrum, redundant half from Hermitian symmetry. */
+GFFT_API gfft_status gfft_nd_forward_full(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src,
+                                          int64_t src_len, void* stream);
+GFFT_API gfft_status gfft_nd_inverse_full(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src,
+                                          int64_t src_len, void* stream);
+GFFT_API gfft_status gfft_nd_forward_host(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src,
+                                          int64_t src_len);
+GFFT_API gfft_status gfft_nd_inverse_host(gfft_plan_nd* plan, void* dst, int64_t dst_len, const void* src,
+                                          int64_t src_len);
+
+/* Batched strided transforms with a 1-D plan: element j of transform b at
+ * b*dist + j*stride in both dst and src (the column batches behind the N-D
+ * plans; plan_strided.go:35-99 for one transform).  Columns (dist = 1,
+ * count <= stride) run one coalesced column kernel. */
+GFFT_API gfft_status gfft_exec_strided_batch(gfft_plan* plan, int32_t direction, void* dst, int64_t dst_len,
+                                             const void* src, int64_t src_len, int64_t count, int64_t stride,
+                                             int64_t dist, void* stream);
+
 /* ---- errors -------------------------------------------------------------- */
 
 /* Text of a status code (the reference's error strings for 1..6). */
