@@ -11,6 +11,8 @@ from .plan import (COMPLEX64, COMPLEX128, KernelAuto, KernelBluestein, KernelDIT
                    KernelSixStep, KernelStockham, NewPlan, NewPlan32, NewPlan64, NewPlanT, NewPlanWithOptions, Plan,
                    PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerMeasure, PlannerPatient)
 
+from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, ConvolveReal, ConvolveRealBatch,
+                       Correlate, Correlate128, CrossCorrelate, CrossCorrelate128)
 from .nd import NewPlan2D, NewPlan3D, NewPlanND, NewPlanReal2D, NewPlanReal3D, PlanND
 from .real import NewPlanReal, NewPlanReal32, NewPlanReal64, NewPlanRealWithOptions, PlanReal
 from .wisdom import (Autotune, ClearWisdom, ExportWisdom, ExportWisdomToString, ImportWisdom,

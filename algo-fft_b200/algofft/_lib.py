@@ -130,6 +130,13 @@ SIGNATURES = {
     "gfft_nd_forward_host": (I32, [P, P, I64, P, I64]),
     "gfft_nd_inverse_host": (I32, [P, P, I64, P, I64]),
     "gfft_exec_strided_batch": (I32, [P, I32, P, I64, P, I64, I64, I64, I64, P]),
+    "gfft_convolve": (I32, [I32, P, I64, P, I64, P, I64, P]),
+    "gfft_correlate": (I32, [I32, P, I64, P, I64, P, I64, P]),
+    "gfft_convolve_real": (I32, [I32, P, I64, P, I64, P, I64, P]),
+    "gfft_convolve_host": (I32, [I32, P, I64, P, I64, P, I64]),
+    "gfft_correlate_host": (I32, [I32, P, I64, P, I64, P, I64]),
+    "gfft_convolve_real_host": (I32, [I32, P, I64, P, I64, P, I64]),
+    "gfft_convolve_real_batch": (I32, [I32, P, I64, P, I64, I64, I64, P, I64, P]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

@@ -264,6 +264,35 @@ GFFT_API gfft_status gfft_exec_strided_batch(gfft_plan* plan, int32_t direction,
                                              const void* src, int64_t src_len, int64_t count, int64_t stride,
                                              int64_t dist, void* stream);
 
+/* ---- convolution and correlation (convolve.go, convolve_real.go, correlate.go) */
+
+/* Convolve / Convolve128 (convolve.go:9,65): dst = a (*) b, complex, length
+ * exactly a_len + b_len - 1 (else GFFT_ERR_LENGTH_MISMATCH); empty inputs ->
+ * GFFT_ERR_INVALID_LENGTH.  Device pointers, ordered on stream. */
+GFFT_API gfft_status gfft_convolve(int32_t precision, void* dst, int64_t dst_len, const void* a, int64_t a_len,
+                                   const void* b, int64_t b_len, void* stream);
+/* CrossCorrelate / Correlate128 (correlate.go:13,48): Convolve with the
+ * conjugate reverse of b; AutoCorrelate is (a, a). */
+GFFT_API gfft_status gfft_correlate(int32_t precision, void* dst, int64_t dst_len, const void* a, int64_t a_len,
+                                    const void* b, int64_t b_len, void* stream);
+/* ConvolveReal (convolve_real.go:9): real inputs (float32 for
+ * GFFT_COMPLEX64, float64 for GFFT_COMPLEX128), FFT length
+ * NextPow2(a_len + b_len - 1). */
+GFFT_API gfft_status gfft_convolve_real(int32_t precision, void* dst, int64_t dst_len, const void* a, int64_t a_len,
+                                        const void* b, int64_t b_len, void* stream);
+GFFT_API gfft_status gfft_convolve_host(int32_t precision, void* dst, int64_t dst_len, const void* a, int64_t a_len,
+                                        const void* b, int64_t b_len);
+GFFT_API gfft_status gfft_correlate_host(int32_t precision, void* dst, int64_t dst_len, const void* a, int64_t a_len,
+                                         const void* b, int64_t b_len);
+GFFT_API gfft_status gfft_convolve_real_host(int32_t precision, void* dst, int64_t dst_len, const void* a,
+                                             int64_t a_len, const void* b, int64_t b_len);
+/* ConvolveReal of `count` signals (a_len reals, a_dist apart) with one kernel
+ * b, results of a_len + b_len - 1 reals dst_dist apart: the reference's
+ * per-signal ConvolveReal loop as one batched computation. */
+GFFT_API gfft_status gfft_convolve_real_batch(int32_t precision, void* dst, int64_t dst_dist, const void* a,
+                                              int64_t a_len, int64_t a_dist, int64_t count, const void* b,
+                                              int64_t b_len, void* stream);
+
 /* ---- errors -------------------------------------------------------------- */
 
 /* Text of a status code (the reference's error strings for 1..6). */
