@@ -15,6 +15,7 @@ from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, C
                        Correlate, Correlate128, CrossCorrelate, CrossCorrelate128)
 from .nd import NewPlan2D, NewPlan3D, NewPlanND, NewPlanReal2D, NewPlanReal3D, PlanND
 from .real import NewPlanReal, NewPlanReal32, NewPlanReal64, NewPlanRealWithOptions, PlanReal
+from .uneven import PlanUneven, uneven_lengths
 from .wisdom import (Autotune, ClearWisdom, ExportWisdom, ExportWisdomToString, ImportWisdom,
                      ImportWisdomFromString, Variants, WisdomLen)
 

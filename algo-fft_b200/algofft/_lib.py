@@ -137,6 +137,11 @@ SIGNATURES = {
     "gfft_correlate_host": (I32, [I32, P, I64, P, I64, P, I64]),
     "gfft_convolve_real_host": (I32, [I32, P, I64, P, I64, P, I64]),
     "gfft_convolve_real_batch": (I32, [I32, P, I64, P, I64, I64, I64, P, I64, P]),
+    "gfft_plan_uneven_new": (I32, [PP, I32, I64, ctypes.POINTER(I64), ctypes.POINTER(PlanOptionsC)]),
+    "gfft_plan_uneven_close": (None, [P]),
+    "gfft_plan_uneven_total": (I64, [P]),
+    "gfft_uneven_exec": (I32, [P, I32, P, P, I32, P]),
+    "gfft_uneven_exec_per_size": (I32, [P, I32, P, P, P]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

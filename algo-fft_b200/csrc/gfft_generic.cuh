@@ -27,6 +27,10 @@ struct GenSched {
 
 __device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
 
+// Thread index handed to gen_fft by threads that own no butterfly: every
+// butterfly index it yields is past the end of every stage.
+constexpr int kIdleThread = 1 << 28;
+
 // Butterflies a thread may hold in one stage of radix R (R*QM <= 32).
 template <int R>
 struct GenQ {
@@ -95,7 +99,7 @@ __global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t 
   if (slot < s.B)
     for (int e = t; e < s.n; e += s.T) x[gpad(e)] = valid ? ld_stream(in + e) : C{0, 0};
   __syncthreads();
-  gen_fft<DIR>(x, s, slot < s.B ? t : s.T, tw);
+  gen_fft<DIR>(x, s, slot < s.B ? t : kIdleThread, tw);
   if (valid) {
     C* out = dst + b * odist;
     for (int e = t; e < s.n; e += s.T) {
@@ -151,7 +155,7 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
   }
   __syncthreads();
   const int slot = tid / s.T, t = tid % s.T;
-  gen_fft<DIR>(base + (slot < NC ? slot : 0) * s.stride, s, slot < NC ? t : s.T, tw);
+  gen_fft<DIR>(base + (slot < NC ? slot : 0) * s.stride, s, slot < NC ? t : kIdleThread, tw);
   if (!valid) return;
   if constexpr (MODE == GEN_PASS1) {
     const C* lo = static_cast<const C*>(bt.lo);
@@ -174,6 +178,34 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
       if constexpr (DIR > 0) v = cscale(v, scale);
       st_stream(out + int64_t(k2) * pitch + col0 + c, v);
     }
+  }
+}
+
+// Chirp w_k = exp(sign * i*pi * k^2 / n) with k^2 reduced mod 2n in exact
+// integer arithmetic before the FP64 evaluation (the reference evaluates
+// float64(k*k)/n, internal/kernels/bluestein.go:20-32, which loses
+// precision as k grows).
+template <typename C>
+__global__ void k_chirp(C* w, int64_t n, int sign) {
+  using Re = typename RealOf<C>::type;
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
+    int64_t m = (k * k) % (2 * n);
+    if (m > n) m -= 2 * n;
+    double s, c;
+    sincospi(double(sign) * double(m) / double(n), &s, &c);
+    w[k] = C{Re(c), Re(s)};
+  }
+}
+
+// b_k = conj(w_k) for k < n, b_{M-k} = conj(w_k) for 0 < k < n, else 0
+// (internal/kernels/bluestein.go:39-58).
+template <typename C>
+__global__ void k_bs_filter_src(C* b, const C* w, int64_t n, int64_t M) {
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < M; j += int64_t(gridDim.x) * blockDim.x) {
+    C v{0, 0};
+    if (j < n) v = cconj(w[j]);
+    else if (M - j < n) v = cconj(w[M - j]);
+    b[j] = v;
   }
 }
 

@@ -55,6 +55,9 @@ struct PlanCore {
 };
 
 bool is_smooth7(int64_t n);
+// Runtime Stockham schedule of a 7-smooth n (false when n is not 7-smooth or
+// needs more than 1024 threads).
+bool make_gen_sched(int64_t n, GenSched* s);
 gfft_status init_generic(PlanCore* c);
 gfft_status init_gen_twopass(PlanCore* c);
 gfft_status init_bluestein(PlanCore* c);

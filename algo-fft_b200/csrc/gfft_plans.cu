@@ -67,6 +67,8 @@ static bool make_sched(int64_t n, GenSched* s) {
 
 static const int kSmemBudget = 200 * 1024;
 
+bool make_gen_sched(int64_t n, GenSched* s) { return make_sched(n, s); }
+
 // --------------------------------------------------------------- launchers
 
 template <typename C>
@@ -248,34 +250,6 @@ gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const 
 }
 
 // ---------------------------------------------------------------- Bluestein
-
-// Chirp w_k = exp(sign * i*pi * k^2 / n) with k^2 reduced mod 2n in exact
-// integer arithmetic before the FP64 evaluation (the reference evaluates
-// float64(k*k)/n, internal/kernels/bluestein.go:20-32, which loses
-// precision as k grows).
-template <typename C>
-__global__ void k_chirp(C* w, int64_t n, int sign) {
-  using Re = typename RealOf<C>::type;
-  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x) {
-    int64_t m = (k * k) % (2 * n);
-    if (m > n) m -= 2 * n;
-    double s, c;
-    sincospi(double(sign) * double(m) / double(n), &s, &c);
-    w[k] = C{Re(c), Re(s)};
-  }
-}
-
-// b_k = conj(w_k) for k < n, b_{M-k} = conj(w_k) for 0 < k < n, else 0
-// (internal/kernels/bluestein.go:39-58).
-template <typename C>
-__global__ void k_bs_filter_src(C* b, const C* w, int64_t n, int64_t M) {
-  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < M; j += int64_t(gridDim.x) * blockDim.x) {
-    C v{0, 0};
-    if (j < n) v = cconj(w[j]);
-    else if (M - j < n) v = cconj(w[M - j]);
-    b[j] = v;
-  }
-}
 
 // work[b][m] = m < n ? x[b][m] * w[m] : 0     (plan_bluestein.go:8-16)
 template <typename C>

@@ -1,0 +1,441 @@
+// Uneven-length batch plans: many transforms of different lengths, packed
+// back to back (transform i at the prefix sum of the lengths before it).
+//
+// The reference has no such entry point: a caller loops Plan.Forward over a
+// plan per length, which is what gfft_uneven_exec_per_size does on the GPU
+// (one launch chain per transform) as the baseline.  gfft_uneven_exec runs
+// the whole batch as:
+//   - every transform that fits one CTA (direct runtime Stockham, or
+//     Bluestein whose FFT length fits) in persistent k_uneven launches, one
+//     per CTA-size class, fed by a device work queue;
+//   - larger power-of-two lengths: gathered into one batch per length, run
+//     through that length's batched plan, scattered back;
+//   - every other larger length through Bluestein, grouped by FFT length M
+//     (NextPow2(2n-1), plan.go:865): one gather (x chirp), one batched FFT_M,
+//     one filter product, one batched inverse FFT_M, one scatter (x chirp).
+// The launch sequence is captured once into a CUDA graph per (direction,
+// dst, src) and replayed.  Plan tables (twiddles, chirps, filters) are built
+// on the GPU at plan creation; filters of one M come from one batched FFT.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+#include "gfft_internal.h"
+#include "gfft_uneven.cuh"
+
+namespace gfft {
+namespace {
+
+struct Group {
+  int64_t M = 0;           // FFT length of the group
+  bool bluestein = false;
+  PlanCore* plan = nullptr;
+  std::vector<BigItem> items;
+  BigItem* d_items = nullptr;
+  void* work = nullptr;    // rows x M
+};
+
+struct Klass {
+  std::vector<UnevenItem> items;
+  UnevenItem* d_items = nullptr;
+  int cta = 0;
+  size_t smem = 0;
+  int grid = 0;
+};
+
+unsigned grid1(int64_t total) { return unsigned(std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 32))); }
+
+const size_t kSmemMax = 200 * 1024;
+
+bool direct_ok(int64_t n, size_t es, GenSched* s) {
+  if (n == 1) {
+    *s = GenSched{};
+    s->n = 1;
+    s->nst = 0;
+    s->T = 1;
+    s->B = 1;
+    s->stride = 1;
+    return true;
+  }
+  return make_gen_sched(n, s) && size_t(s->stride) * es <= kSmemMax;
+}
+
+template <typename C>
+cudaError_t set_uneven_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(&k_uneven<C, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(&k_uneven<C, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax));
+  return e;
+}
+
+}  // namespace
+}  // namespace gfft
+
+using namespace gfft;
+
+struct gfft_plan_uneven {
+  int prec = 0;
+  int device = 0;
+  int64_t count = 0, total = 0;
+  std::vector<int64_t> len, off;
+  void* tab = nullptr;
+  std::vector<UnevenDesc> descs;
+  UnevenDesc* d_descs = nullptr;
+  Klass klass[2];
+  std::vector<Group> groups;
+  unsigned* counters = nullptr;
+  std::map<int64_t, PlanCore*> single;  // per-length plans of the per-size path
+  std::mutex mu;
+  struct Graph {
+    int dir;
+    const void* src;
+    void* dst;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Graph> graphs;
+  cudaStream_t cap = nullptr;
+};
+
+extern "C" GFFT_API void gfft_plan_uneven_close(gfft_plan_uneven* p);
+
+namespace gfft {
+
+static gfft_status uneven_build(gfft_plan_uneven* p) {
+  const size_t es = elem_bytes(p->prec);
+  const int64_t max_direct_bs = p->prec == kC64 ? 16384 : 8192;
+  // distinct lengths and their handling
+  std::map<int64_t, int> desc_of;                 // small lengths -> descriptor
+  std::map<int64_t, std::vector<int64_t>> bs_by_m;  // Bluestein lengths per FFT length M
+  std::map<int64_t, int64_t> tw_off;              // W_L table offsets
+  std::map<int64_t, int64_t> chirp_off, filt_off;
+  std::map<int64_t, int> big_pow2_group;          // large pow2 length -> group
+  std::map<int64_t, int> big_bs_group;            // M -> group
+  int64_t cursor = 0;
+  auto alloc = [&](int64_t n) {
+    const int64_t at = cursor;
+    cursor += (n + 1) & ~int64_t(1);  // keep every table 16-byte aligned
+    return at;
+  };
+  std::vector<int64_t> distinct(p->len);
+  std::sort(distinct.begin(), distinct.end());
+  distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+  for (int64_t n : distinct) {
+    GenSched s;
+    if (direct_ok(n, es, &s)) {
+      UnevenDesc d{};
+      d.s = s;
+      d.n = n;
+      d.bluestein = 0;
+      if (!tw_off.count(n)) tw_off[n] = alloc(n);
+      d.tw = tw_off[n];
+      desc_of[n] = int(p->descs.size());
+      p->descs.push_back(d);
+      continue;
+    }
+    if ((n & (n - 1)) == 0) {
+      big_pow2_group[n] = int(p->groups.size());
+      Group g;
+      g.M = n;
+      p->groups.push_back(g);
+      continue;
+    }
+    int64_t M = 1;
+    while (M < 2 * n - 1) M <<= 1;
+    bs_by_m[M].push_back(n);
+    chirp_off[n] = alloc(n);
+    GenSched sm;
+    if (M <= max_direct_bs && direct_ok(M, es, &sm)) {
+      UnevenDesc d{};
+      d.s = sm;
+      d.n = n;
+      d.bluestein = 1;
+      if (!tw_off.count(M)) tw_off[M] = alloc(M);
+      d.tw = tw_off[M];
+      d.chirp = chirp_off[n];
+      desc_of[n] = int(p->descs.size());
+      p->descs.push_back(d);
+    } else if (!big_bs_group.count(M)) {
+      big_bs_group[M] = int(p->groups.size());
+      Group g;
+      g.M = M;
+      g.bluestein = true;
+      p->groups.push_back(g);
+    }
+  }
+  // filters: one contiguous block of rows per M, in bs_by_m order
+  for (auto& kv : bs_by_m)
+    for (int64_t n : kv.second) filt_off[n] = alloc(kv.first);
+  for (auto& d : p->descs)
+    if (d.bluestein) d.filt = filt_off[d.n];
+  GFFT_CUDA(cudaMalloc(&p->tab, size_t(std::max<int64_t>(cursor, 1)) * es));
+  char* tab = static_cast<char*>(p->tab);
+  for (auto& kv : tw_off) {
+    gfft_status s = fill_twiddles(p->prec, tab + kv.second * es, kv.first, kv.first, 1, 0);
+    if (s != GFFT_OK) return s;
+  }
+  for (auto& kv : chirp_off) {
+    const int64_t n = kv.first;
+    if (p->prec == kC64)
+      k_chirp<float2><<<grid1(n), 256>>>(reinterpret_cast<float2*>(tab + kv.second * es), n, -1);
+    else
+      k_chirp<double2><<<grid1(n), 256>>>(reinterpret_cast<double2*>(tab + kv.second * es), n, -1);
+  }
+  GFFT_CUDA(cudaGetLastError());
+  for (auto& kv : bs_by_m) {
+    const int64_t M = kv.first;
+    for (int64_t n : kv.second) {
+      if (p->prec == kC64)
+        k_bs_filter_src<float2><<<grid1(M), 256>>>(reinterpret_cast<float2*>(tab + filt_off[n] * es),
+                                                    reinterpret_cast<const float2*>(tab + chirp_off[n] * es), n, M);
+      else
+        k_bs_filter_src<double2><<<grid1(M), 256>>>(reinterpret_cast<double2*>(tab + filt_off[n] * es),
+                                                     reinterpret_cast<const double2*>(tab + chirp_off[n] * es), n, M);
+    }
+    GFFT_CUDA(cudaGetLastError());
+    PlanCore pc;
+    gfft_status s = core_init(&pc, p->prec, M, p->device);
+    if (s == GFFT_OK)
+      s = core_exec(&pc, -1, tab + filt_off[kv.second.front()] * es, tab + filt_off[kv.second.front()] * es,
+                    int64_t(kv.second.size()), M, M, 0);
+    GFFT_CUDA(cudaStreamSynchronize(0));
+    core_free(&pc);
+    if (s != GFFT_OK) return s;
+  }
+  // items
+  for (int64_t i = 0; i < p->count; ++i) {
+    const int64_t n = p->len[i];
+    auto it = desc_of.find(n);
+    if (it != desc_of.end()) {
+      const UnevenDesc& d = p->descs[it->second];
+      Klass& k = p->klass[d.s.T <= 128 ? 0 : 1];
+      k.items.push_back(UnevenItem{p->off[i], it->second, 0});
+      continue;
+    }
+    if ((n & (n - 1)) == 0) {
+      p->groups[big_pow2_group[n]].items.push_back(BigItem{p->off[i], n, 0, 0});
+    } else {
+      int64_t M = 1;
+      while (M < 2 * n - 1) M <<= 1;
+      p->groups[big_bs_group[M]].items.push_back(BigItem{p->off[i], n, chirp_off[n], filt_off[n]});
+    }
+  }
+  // queue order: most expensive first (longest-first list schedule)
+  auto cost = [&](const UnevenItem& u) {
+    const UnevenDesc& d = p->descs[u.desc];
+    return double(d.s.n) * std::log2(double(d.s.n) + 1.0) * (d.bluestein ? 2.0 : 1.0);
+  };
+  int dev = 0, sms = 0;
+  GFFT_CUDA(cudaGetDevice(&dev));
+  GFFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GFFT_CUDA(p->prec == kC64 ? set_uneven_attrs<float2>() : set_uneven_attrs<double2>());
+  for (Klass& k : p->klass) {
+    if (k.items.empty()) continue;
+    std::stable_sort(k.items.begin(), k.items.end(),
+                     [&](const UnevenItem& a, const UnevenItem& b) { return cost(a) > cost(b); });
+    int maxT = 32;
+    size_t smem = 0;
+    for (const auto& u : k.items) {
+      maxT = std::max(maxT, p->descs[u.desc].s.T);
+      smem = std::max(smem, size_t(p->descs[u.desc].s.stride) * es);
+    }
+    k.cta = std::min(1024, (maxT + 31) / 32 * 32);
+    k.smem = smem;
+    int occ = 0;
+    const void* fn = p->prec == kC64 ? reinterpret_cast<const void*>(&k_uneven<float2, -1>)
+                                     : reinterpret_cast<const void*>(&k_uneven<double2, -1>);
+    GFFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, k.cta, k.smem));
+    k.grid = int(std::min<int64_t>(int64_t(k.items.size()), int64_t(sms) * std::max(occ, 1)));
+    GFFT_CUDA(cudaMalloc(&k.d_items, k.items.size() * sizeof(UnevenItem)));
+    GFFT_CUDA(cudaMemcpy(k.d_items, k.items.data(), k.items.size() * sizeof(UnevenItem), cudaMemcpyHostToDevice));
+  }
+  if (!p->descs.empty()) {
+    GFFT_CUDA(cudaMalloc(&p->d_descs, p->descs.size() * sizeof(UnevenDesc)));
+    GFFT_CUDA(cudaMemcpy(p->d_descs, p->descs.data(), p->descs.size() * sizeof(UnevenDesc), cudaMemcpyHostToDevice));
+  }
+  for (Group& g : p->groups) {
+    g.plan = new (std::nothrow) PlanCore;
+    if (!g.plan) return GFFT_ERR_OUT_OF_MEMORY;
+    gfft_status s = core_init(g.plan, p->prec, g.M, p->device);
+    if (s != GFFT_OK) return s;
+    GFFT_CUDA(cudaMalloc(&g.d_items, g.items.size() * sizeof(BigItem)));
+    GFFT_CUDA(cudaMemcpy(g.d_items, g.items.data(), g.items.size() * sizeof(BigItem), cudaMemcpyHostToDevice));
+    GFFT_CUDA(cudaMalloc(&g.work, g.items.size() * size_t(g.M) * es));
+  }
+  GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
+  GFFT_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+  return GFFT_OK;
+}
+
+template <typename C, int DIR>
+static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStream_t st) {
+  GFFT_CUDA(cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned), st));
+  for (int k = 0; k < 2; ++k) {
+    const Klass& K = p->klass[k];
+    if (K.items.empty()) continue;
+    k_uneven<C, DIR><<<K.grid, K.cta, K.smem, st>>>(src, dst, K.d_items, int(K.items.size()), p->d_descs,
+                                                    static_cast<const C*>(p->tab), p->counters + k);
+    GFFT_CUDA(cudaGetLastError());
+  }
+  for (Group& g : p->groups) {
+    const int64_t rows = int64_t(g.items.size());
+    if (rows == 0) continue;
+    C* work = static_cast<C*>(g.work);
+    const C* tab = static_cast<const C*>(p->tab);
+    k_big_gather<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(work, g.M, src, g.d_items, rows, tab, g.bluestein);
+    GFFT_CUDA(cudaGetLastError());
+    if (!g.bluestein) {
+      gfft_status s = core_exec(g.plan, DIR, work, work, rows, g.M, g.M, st);
+      if (s != GFFT_OK) return s;
+    } else {
+      gfft_status s = core_exec(g.plan, -1, work, work, rows, g.M, g.M, st);
+      if (s != GFFT_OK) return s;
+      k_big_filter<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(work, g.M, g.d_items, rows, tab);
+      GFFT_CUDA(cudaGetLastError());
+      s = core_exec(g.plan, +1, work, work, rows, g.M, g.M, st);  // includes 1/M
+      if (s != GFFT_OK) return s;
+    }
+    k_big_scatter<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(dst, work, g.M, g.d_items, rows, tab, g.bluestein);
+    GFFT_CUDA(cudaGetLastError());
+  }
+  return GFFT_OK;
+}
+
+static gfft_status uneven_dispatch(gfft_plan_uneven* p, int dir, void* dst, const void* src, cudaStream_t st) {
+  if (p->prec == kC64)
+    return dir < 0 ? uneven_run<float2, -1>(p, static_cast<float2*>(dst), static_cast<const float2*>(src), st)
+                   : uneven_run<float2, +1>(p, static_cast<float2*>(dst), static_cast<const float2*>(src), st);
+  return dir < 0 ? uneven_run<double2, -1>(p, static_cast<double2*>(dst), static_cast<const double2*>(src), st)
+                 : uneven_run<double2, +1>(p, static_cast<double2*>(dst), static_cast<const double2*>(src), st);
+}
+
+}  // namespace gfft
+
+extern "C" {
+
+gfft_status gfft_plan_uneven_new(gfft_plan_uneven** out, int32_t precision, int64_t count, const int64_t* lengths,
+                                 const gfft_plan_options* opts) {
+  clear_error();
+  if (!out) return GFFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (count < 1 || !lengths) return GFFT_ERR_INVALID_LENGTH;
+  if (precision != GFFT_COMPLEX64 && precision != GFFT_COMPLEX128) return GFFT_ERR_INVALID_ARGUMENT;
+  for (int64_t i = 0; i < count; ++i)
+    if (lengths[i] < 1 || lengths[i] > (int64_t(1) << 24)) {
+      set_error("transform " + std::to_string(i) + " has an unsupported length");
+      return GFFT_ERR_INVALID_LENGTH;
+    }
+  gfft_plan_options o{};
+  if (opts) o = *opts;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
+  GFFT_CUDA(cudaSetDevice(o.device));
+  auto* p = new (std::nothrow) gfft_plan_uneven;
+  if (!p) return GFFT_ERR_OUT_OF_MEMORY;
+  p->prec = precision;
+  p->device = o.device;
+  p->count = count;
+  p->len.assign(lengths, lengths + count);
+  p->off.resize(count);
+  for (int64_t i = 0; i < count; ++i) {
+    p->off[i] = p->total;
+    p->total += lengths[i];
+  }
+  gfft_status s = uneven_build(p);
+  if (s != GFFT_OK) {
+    gfft_plan_uneven_close(p);
+    return s;
+  }
+  *out = p;
+  return GFFT_OK;
+}
+
+void gfft_plan_uneven_close(gfft_plan_uneven* p) {
+  if (!p) return;
+  for (auto& g : p->graphs) cudaGraphExecDestroy(g.exec);
+  for (Klass& k : p->klass)
+    if (k.d_items) cudaFree(k.d_items);
+  for (Group& g : p->groups) {
+    if (g.plan) {
+      core_free(g.plan);
+      delete g.plan;
+    }
+    if (g.d_items) cudaFree(g.d_items);
+    if (g.work) cudaFree(g.work);
+  }
+  for (auto& kv : p->single) {
+    core_free(kv.second);
+    delete kv.second;
+  }
+  if (p->d_descs) cudaFree(p->d_descs);
+  if (p->tab) cudaFree(p->tab);
+  if (p->counters) cudaFree(p->counters);
+  if (p->cap) cudaStreamDestroy(p->cap);
+  delete p;
+}
+
+int64_t gfft_plan_uneven_total(const gfft_plan_uneven* p) { return p ? p->total : 0; }
+
+gfft_status gfft_uneven_exec(gfft_plan_uneven* p, int32_t direction, void* dst, const void* src, int32_t use_graph,
+                             void* stream) {
+  clear_error();
+  if (!p) return GFFT_ERR_INVALID_ARGUMENT;
+  if (!dst || !src) return GFFT_ERR_NIL_SLICE;
+  if (direction != -1 && direction != 1) return GFFT_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> g(p->mu);  // the plan's work buffers are shared
+  if (!use_graph) return uneven_dispatch(p, direction, dst, src, st);
+  cudaGraphExec_t exec = nullptr;
+  for (auto& gr : p->graphs)
+    if (gr.dir == direction && gr.src == src && gr.dst == dst) exec = gr.exec;
+  if (!exec) {
+    cudaGraph_t graph = nullptr;
+    GFFT_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    gfft_status s = uneven_dispatch(p, direction, dst, src, p->cap);
+    cudaError_t e = cudaStreamEndCapture(p->cap, &graph);
+    if (s != GFFT_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
+    }
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    p->graphs.push_back({direction, src, dst, exec});
+  }
+  GFFT_CUDA(cudaGraphLaunch(exec, st));
+  return GFFT_OK;
+}
+
+gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* p, int32_t direction, void* dst, const void* src,
+                                      void* stream) {
+  clear_error();
+  if (!p) return GFFT_ERR_INVALID_ARGUMENT;
+  if (!dst || !src) return GFFT_ERR_NIL_SLICE;
+  if (direction != -1 && direction != 1) return GFFT_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> g(p->mu);
+  const size_t es = elem_bytes(p->prec);
+  for (int64_t i = 0; i < p->count; ++i) {
+    const int64_t n = p->len[i];
+    auto it = p->single.find(n);
+    if (it == p->single.end()) {
+      auto* c = new (std::nothrow) PlanCore;
+      if (!c) return GFFT_ERR_OUT_OF_MEMORY;
+      gfft_status s = core_init(c, p->prec, n, p->device);
+      if (s != GFFT_OK) {
+        core_free(c);
+        delete c;
+        return s;
+      }
+      it = p->single.emplace(n, c).first;
+    }
+    gfft_status s = core_exec(it->second, direction, static_cast<char*>(dst) + size_t(p->off[i]) * es,
+                              static_cast<const char*>(src) + size_t(p->off[i]) * es, 1, n, n, st);
+    if (s != GFFT_OK) return s;
+  }
+  return GFFT_OK;
+}
+
+}  // extern "C"

@@ -293,6 +293,31 @@ GFFT_API gfft_status gfft_convolve_real_batch(int32_t precision, void* dst, int6
                                               int64_t a_len, int64_t a_dist, int64_t count, const void* b,
                                               int64_t b_len, void* stream);
 
+/* ---- uneven-length batches ------------------------------------------------ */
+
+/* No single reference entry point: a Go caller loops Plan.Forward over one
+ * plan per length.  A plan for `count` transforms of the given lengths
+ * (1 .. 2^24 each), packed back to back: transform i starts at the sum of
+ * the lengths before it.  Plan creation builds every twiddle, chirp and
+ * Bluestein filter on the GPU. */
+typedef struct gfft_plan_uneven gfft_plan_uneven;
+GFFT_API gfft_status gfft_plan_uneven_new(gfft_plan_uneven** out, int32_t precision, int64_t count,
+                                          const int64_t* lengths, const gfft_plan_options* opts);
+GFFT_API void gfft_plan_uneven_close(gfft_plan_uneven* plan);
+/* Total elements of the packed batch (sum of the lengths). */
+GFFT_API int64_t gfft_plan_uneven_total(const gfft_plan_uneven* plan);
+/* The whole batch in a few launches (persistent work-queue kernel for
+ * every transform that fits one CTA, grouped batches for the rest),
+ * replayed from a CUDA graph captured on first use per (direction, dst,
+ * src) when use_graph is set.  dst may equal src.  Calls on one plan are
+ * serialized (they share its work buffers). */
+GFFT_API gfft_status gfft_uneven_exec(gfft_plan_uneven* plan, int32_t direction, void* dst, const void* src,
+                                      int32_t use_graph, void* stream);
+/* The plain per-size path: one plan per distinct length and one transform
+ * call per transform, as a loop over Plan.Forward would do. */
+GFFT_API gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* plan, int32_t direction, void* dst,
+                                               const void* src, void* stream);
+
 /* ---- errors -------------------------------------------------------------- */
 
 /* Text of a status code (the reference's error strings for 1..6). */
