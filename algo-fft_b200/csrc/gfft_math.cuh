@@ -212,6 +212,26 @@ __device__ __forceinline__ C big_twiddle(const BigTwiddle& bt, int64_t m) {
 }
 
 // Streaming global accesses: the batch is touched exactly once.
+// Asks the TMA unit to bring [p, p + bytes) into L2 ahead of its use (no
+// registers, no completion to wait for).  p and bytes must be multiples of
+// 16; callers check both.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Prefetches [p, p + bytes) in runs of at most 32 KB spread over the
+// calling threads (thread `lane` of `nthr`); skipped unless p and bytes are
+// multiples of 16.
+__device__ __forceinline__ void prefetch_range(const void* p, int64_t bytes, int lane, int nthr) {
+  if ((bytes & 15) || (reinterpret_cast<uintptr_t>(p) & 15)) return;
+  constexpr int64_t kRun = 32768;
+  const int64_t runs = (bytes + kRun - 1) / kRun;
+  for (int64_t i = lane; i < runs; i += nthr) {
+    const int64_t len = bytes - i * kRun < kRun ? bytes - i * kRun : kRun;
+    prefetch_l2(static_cast<const char*>(p) + i * kRun, unsigned(len));
+  }
+}
+
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
 __device__ __forceinline__ void st_stream(float2* p, float2 v) { __stcs(p, v); }

@@ -146,11 +146,28 @@ struct GlobalStore {
 // Batched C2C: transform b reads src[b*idist .. b*idist+N) and writes
 // dst[b*odist ..).  src may equal dst (every CTA reads its whole transform
 // before it writes any of it).  tw holds W_N^m, m < N.
+//
+// With ahead > 0 each CTA first asks for the input of CTA blockIdx + ahead
+// to be prefetched into L2 (ahead = the number of co-resident CTAs, so the
+// data arrives about one CTA lifetime before it is read): HBM keeps
+// streaming while the SM's few resident CTAs are in their compute and
+// store phases.  Prefetching only reads, so in-place calls use it too.
 template <typename C, int N, int EPT, int DIR>
 __global__ void __launch_bounds__(Pow2Shape<N, EPT, sizeof(C)>::TPB)
 k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const C* __restrict__ tw,
-       typename RealOf<C>::type scale) {
+       typename RealOf<C>::type scale, int64_t ahead) {
   using S = Pow2Shape<N, EPT, sizeof(C)>;
+  if (ahead > 0) {
+    const int64_t b2 = (int64_t(blockIdx.x) + ahead) * S::B;
+    if (b2 < count) {
+      const int nb = int(count - b2 < S::B ? count - b2 : S::B);
+      if (idist == N)
+        prefetch_range(src + b2 * idist, int64_t(nb) * N * int64_t(sizeof(C)), threadIdx.x, S::TPB);
+      else
+        for (int j = 0; j < nb; ++j)
+          prefetch_range(src + (b2 + j) * idist, int64_t(N) * int64_t(sizeof(C)), threadIdx.x, S::TPB);
+    }
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sh = reinterpret_cast<C*>(smem_raw) + (threadIdx.x / S::T) * S::STRIDE;
   const int t = threadIdx.x % S::T;
