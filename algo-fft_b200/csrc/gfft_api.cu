@@ -34,7 +34,7 @@ static gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, i
   cudaStream_t st = nullptr;
   GFFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   void* d = nullptr;
-  cudaError_t e = cudaMallocAsync(&d, bytes, st);
+  cudaError_t e = ws_alloc(reinterpret_cast<void**>(&d), bytes, st);
   gfft_status s = GFFT_OK;
   if (e != cudaSuccess) {
     s = cuda_status(e, "cudaMallocAsync");
@@ -202,7 +202,7 @@ static gfft_status do_strided(gfft_plan* p, int dir, void* dst, int64_t dst_len,
   cudaStream_t st = as_stream(stream);
   const size_t es = elem_bytes(p->core.prec);
   void* tmp = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&tmp, size_t(n) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&tmp), size_t(n) * es, st));
   cudaError_t e = cudaMemcpy2DAsync(tmp, es, src, size_t(stride) * es, es, size_t(n), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess) {
     s = core_exec(&p->core, dir, tmp, tmp, 1, n, n, st);

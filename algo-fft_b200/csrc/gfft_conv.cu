@@ -106,7 +106,7 @@ static gfft_status convolve_dev(int prec, C* dst, const C* a, int64_t na, const 
   gfft_status s = cached_plan(prec, L, &p);
   if (s != GFFT_OK) return s;
   C* work = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&work, size_t(2 * L) * sizeof(C), st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&work), size_t(2 * L) * sizeof(C), st));
   k_pad<C><<<grid1(L), 256, 0, st>>>(work, L, a, na, 0, 1, false);
   if (correlate)
     k_pad_conj<C><<<grid1(L), 256, 0, st>>>(work + L, L, b, nb);
@@ -140,7 +140,7 @@ static gfft_status convolve_real_dev(int prec, R* dst, int64_t dst_dist, const R
   // [count + 1 padded rows of F reals | count + 1 spectra of h1 bins]
   R* pad = nullptr;
   const size_t pad_bytes = size_t(count + 1) * size_t(F) * sizeof(R);
-  GFFT_CUDA(cudaMallocAsync(&pad, pad_bytes + size_t(count + 1) * size_t(h1) * sizeof(C), st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&pad), pad_bytes + size_t(count + 1) * size_t(h1) * sizeof(C), st));
   C* spec = reinterpret_cast<C*>(reinterpret_cast<char*>(pad) + pad_bytes);
   k_pad<R><<<grid1(count * F), 256, 0, st>>>(pad, F, a, na, a_dist, count, false);
   k_pad<R><<<grid1(F), 256, 0, st>>>(pad + count * F, F, b, nb, 0, 1, false);

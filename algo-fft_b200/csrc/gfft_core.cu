@@ -1,5 +1,6 @@
 // Kernel registry, device twiddle generation and the 1-D schedule choice.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <mutex>
 #include <vector>
@@ -69,8 +70,10 @@ cudaError_t prepare_kernels() {
   }
   for (const auto& k : twopass_table()) {
     if (k.smem > 48 * 1024) {
-      e = cudaFuncSetAttribute(k.func, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
-      if (e != cudaSuccess) return e;
+      for (const void* f : {k.func, k.split_func[0], k.split_func[1]}) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+        if (e != cudaSuccess) return e;
+      }
     }
   }
   done.push_back(dev);
@@ -117,6 +120,39 @@ gfft_status make_twiddles(int prec, int64_t n, void** out, cudaStream_t st) {
   }
   *out = p;
   return GFFT_OK;
+}
+
+// ---------------------------------------------------------------- workspace
+
+// Per-call workspace (two-pass scratch, Bluestein and N-D temporaries, host
+// staging) comes from one stream-ordered pool per device that keeps freed
+// memory (release threshold = max): the device's default pool returns its
+// memory at every synchronize, so each call would map its workspace anew.
+cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t st) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, cudaMemPool_t>> pools;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& kv : pools)
+      if (kv.first == dev) pool = kv.second;
+    if (!pool) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pool, &props);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = ~uint64_t(0);
+      e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+      pools.emplace_back(dev, pool);
+    }
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
 
 // ---------------------------------------------------------------- copy kernel
@@ -315,43 +351,37 @@ void core_free(PlanCore* c) {
   c->algo = Algo::Trivial;
 }
 
+// Two-pass execution in the split schedule (k_tp_split): per chunk of up to
+// 1 GiB of intermediate, one pass-1 launch and one pass-2 launch.  The
+// scratch comes from the library's workspace pool.
 static gfft_status exec_twopass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
                                 int64_t idist, int64_t odist, cudaStream_t st) {
   const TwoPassKernel* k = c->tp[dir < 0 ? 0 : 1];
-  const size_t es = elem_bytes(c->prec);
-  const int groups = int((count + c->group - 1) / c->group);
-  const size_t ctr_bytes = (size_t(1) + 2 * size_t(groups)) * sizeof(unsigned);
-  const size_t ctr_pad = (ctr_bytes + 255) & ~size_t(255);
-  const size_t scratch_bytes = size_t(c->slots) * size_t(c->group) * size_t(c->n) * es;
+  const int64_t tbytes = c->n * int64_t(elem_bytes(c->prec));
+  const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(1) << 30) / tbytes));
   void* ws = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&ws, ctr_pad + scratch_bytes, st));
-  cudaError_t e = cudaMemsetAsync(ws, 0, ctr_bytes, st);
-  if (e == cudaSuccess) {
-    TwoPassParams p;
-    p.src = src;
-    p.dst = dst;
-    p.scratch = static_cast<char*>(ws) + ctr_pad;
-    p.count = count;
-    p.idist = idist;
-    p.odist = odist;
-    p.tw1 = c->tw1;
-    p.tw2 = c->tw2;
-    p.bt.lo = c->bt_lo;
-    p.bt.hi = c->bt_hi;
-    p.bt.shift = c->bt_shift;
-    p.ctr = static_cast<unsigned*>(ws);
-    p.status = c->status;
-    p.groups = groups;
-    p.G = c->group;
-    p.S = c->slots;
-    p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
-    p.spin_limit = 1u << 24;
-    const int64_t tiles = int64_t(groups) * c->group * ((k->n2 / k->nc1) + (k->n1 / k->nc2));
-    const int grid = int(std::min<int64_t>(tiles, c->resident));
-    e = k->launch(p, grid, st);
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&ws), size_t(nb) * size_t(tbytes), st));
+  TwoPassParams p{};
+  p.src = src;
+  p.dst = dst;
+  p.scratch = ws;
+  p.count = count;
+  p.idist = idist;
+  p.odist = odist;
+  p.tw1 = c->tw1;
+  p.tw2 = c->tw2;
+  p.bt.lo = c->bt_lo;
+  p.bt.hi = c->bt_hi;
+  p.bt.shift = c->bt_shift;
+  p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+  cudaError_t e = cudaSuccess;
+  for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += nb) {
+    const int64_t m = std::min(nb, count - b0);
+    e = k->split(p, 1, b0, m, st);
+    if (e == cudaSuccess) e = k->split(p, 2, b0, m, st);
   }
   cudaFreeAsync(ws, st);
-  if (e != cudaSuccess) return cuda_status(e, "k_twopass");
+  if (e != cudaSuccess) return cuda_status(e, "k_tp_split");
   return GFFT_OK;
 }
 

@@ -69,6 +69,9 @@ gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void*
                               int64_t odist, cudaStream_t st);
 
 // Fills dst[j] = W_n^{(j*step) mod n} for j < count (FP64, rounded).
+// Stream-ordered workspace from the library's per-device pool (released
+// with cudaFreeAsync; the pool keeps the memory for later calls).
+cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t st);
 gfft_status fill_twiddles(int prec, void* dst, int64_t n, int64_t count, int64_t step, cudaStream_t st);
 
 // Chooses and prepares the schedule of a 1-D complex transform of length n:

@@ -122,7 +122,7 @@ static gfft_status axis_exec(const Axis& a, int prec, int dir, void* out, const 
   // transpose [n][inner] -> [inner][n], rows, transpose back
   const size_t es = elem_bytes(prec);
   void* tmp = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&tmp, size_t(a.outer) * size_t(block) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&tmp), size_t(a.outer) * size_t(block) * es, st));
   gfft_status s = GFFT_OK;
   for (int64_t r = 0; r < reps && s == GFFT_OK; ++r) {
     const size_t off = size_t(r) * size_t(dist) * es;
@@ -323,7 +323,7 @@ static gfft_status nd_forward(gfft_plan_nd* p, bool full, void* dst, const void*
   int64_t cdist = dout;
   void* tmp = nullptr;
   if (full) {
-    GFFT_CUDA(cudaMallocAsync(&tmp, size_t(reps) * size_t(p->clen) * es, st));
+    GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&tmp), size_t(reps) * size_t(p->clen) * es, st));
     comp = tmp;
     cdist = p->clen;
   }
@@ -354,7 +354,7 @@ static gfft_status nd_inverse(gfft_plan_nd* p, bool full, void* dst, const void*
   const size_t es = elem_bytes(p->prec);
   const int64_t n = p->dims[p->nd - 1], h1 = n / 2 + 1, rows = p->len / n;
   void* tmp = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&tmp, size_t(reps) * size_t(p->clen) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&tmp), size_t(reps) * size_t(p->clen) * es, st));
   cudaError_t e = cudaSuccess;
   if (full) {
     if (p->prec == kC64)
@@ -411,8 +411,8 @@ static gfft_status nd_host(gfft_plan_nd* p, bool inverse, bool full, void* dst, 
   GFFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   void *ds = nullptr, *dd = nullptr;
   gfft_status s = GFFT_OK;
-  cudaError_t e = cudaMallocAsync(&ds, sb ? sb : 1, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&dd, db ? db : 1, st);
+  cudaError_t e = ws_alloc(reinterpret_cast<void**>(&ds), sb ? sb : 1, st);
+  if (e == cudaSuccess) e = ws_alloc(reinterpret_cast<void**>(&dd), db ? db : 1, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ds, src, sb, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dd, dst, db, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
@@ -483,7 +483,7 @@ gfft_status gfft_exec_strided_batch(gfft_plan* plan, int32_t direction, void* ds
     GenSched cs;
     if (column_sched(n, prec, &cs)) {
       void* w = nullptr;
-      GFFT_CUDA(cudaMallocAsync(&w, size_t(n) * elem_bytes(prec), st));
+      GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&w), size_t(n) * elem_bytes(prec), st));
       gfft_status s = fill_twiddles(prec, w, n, n, 1, st);
       if (s == GFFT_OK) s = exec_columns(cs, prec, direction, dst, src, 1, 0, count, stride, w, st);
       cudaFreeAsync(w, st);
@@ -493,7 +493,7 @@ gfft_status gfft_exec_strided_batch(gfft_plan* plan, int32_t direction, void* ds
   // general layout: gather into rows, transform, scatter back
   const size_t es = elem_bytes(prec);
   void* tmp = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&tmp, size_t(count) * size_t(n) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&tmp), size_t(count) * size_t(n) * es, st));
   cudaError_t e = cudaSuccess;
   for (int64_t b = 0; b < count && e == cudaSuccess; ++b)
     e = cudaMemcpy2DAsync(static_cast<char*>(tmp) + size_t(b) * size_t(n) * es, es,

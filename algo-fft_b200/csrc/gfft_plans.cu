@@ -209,7 +209,7 @@ static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const
   const int64_t n = c->n;
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(64) << 20) / (n * int64_t(es))));
   void* scratch = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&scratch, size_t(chunk) * size_t(n) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&scratch), size_t(chunk) * size_t(n) * es, st));
   BigTwiddle bt{c->bt_lo, c->bt_hi, c->bt_shift};
   const double scale = 1.0 / double(n);
   cudaError_t e = cudaSuccess;
@@ -331,7 +331,7 @@ static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const v
   const int d = dir < 0 ? 0 : 1;
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
   void* work = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&work, size_t(chunk) * size_t(M) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&work), size_t(chunk) * size_t(M) * es, st));
   gfft_status s = GFFT_OK;
   cudaError_t e = cudaSuccess;
   const double scale = dir < 0 ? 1.0 : 1.0 / double(n);

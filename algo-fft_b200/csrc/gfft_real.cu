@@ -224,7 +224,7 @@ gfft_status real_forward(gfft_plan_real* p, int scaling, void* dst, const void* 
     return GFFT_OK;
   }
   void* z = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&z, size_t(batch) * size_t(p->h) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&z), size_t(batch) * size_t(p->h) * es, st));
   const unsigned g = grid1(batch * (p->h + 1));
   if (p->prec == kC64)
     k_pack_real<float2><<<g, 256, 0, st>>>(static_cast<float2*>(z), static_cast<const float*>(src), p->h, batch, sr);
@@ -271,7 +271,7 @@ gfft_status real_inverse(gfft_plan_real* p, void* dst, const void* src, int64_t 
     return GFFT_OK;
   }
   void* z = nullptr;
-  GFFT_CUDA(cudaMallocAsync(&z, size_t(batch) * size_t(p->h) * es, st));
+  GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&z), size_t(batch) * size_t(p->h) * es, st));
   const unsigned g = grid1(batch * p->h);
   if (p->prec == kC64)
     k_c2r_pre<float2><<<g, 256, 0, st>>>(static_cast<float2*>(z), static_cast<const float2*>(src),
@@ -301,8 +301,8 @@ static gfft_status real_host(gfft_plan_real* p, bool inverse, int scaling, void*
   GFFT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   void *ds = nullptr, *dd = nullptr;
   gfft_status s = GFFT_OK;
-  cudaError_t e = cudaMallocAsync(&ds, size_t(src_bytes), st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&dd, size_t(dst_bytes), st);
+  cudaError_t e = ws_alloc(reinterpret_cast<void**>(&ds), size_t(src_bytes), st);
+  if (e == cudaSuccess) e = ws_alloc(reinterpret_cast<void**>(&dd), size_t(dst_bytes), st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ds, src, size_t(src_bytes), cudaMemcpyHostToDevice, st);
   // the parts of dst outside the transforms keep the caller's values
   if (e == cudaSuccess) e = cudaMemcpyAsync(dd, dst, size_t(dst_bytes), cudaMemcpyHostToDevice, st);

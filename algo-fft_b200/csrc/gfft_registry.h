@@ -30,6 +30,8 @@ struct TwoPassKernel {
   int te = 0, emax = 0;  // variant: tile elements, max elements per thread
   const void* func;
   cudaError_t (*launch)(const TwoPassParams& p, int grid, cudaStream_t st);
+  const void* split_func[2];  // k_tp_split pass 1, pass 2
+  cudaError_t (*split)(const TwoPassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st);
 };
 
 void register_pow2(const Pow2Kernel& k);

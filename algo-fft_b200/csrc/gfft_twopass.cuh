@@ -307,4 +307,56 @@ k_twopass(TwoPassParams p) {
   }
 }
 
+// Split form (the default schedule): one plain launch per pass over a chunk
+// of transforms starting at b0, one tile per CTA, no cross-CTA waits.  Pass
+// 1 writes the chunk's intermediate to scratch (the chunk's size); pass 2
+// reads it back; the two launches are stream-ordered.  Measured on B200 it
+// beats the persistent form above at every size, although its intermediate
+// makes a round trip through HBM: the persistent form loses more to the
+// three serialized L2 round trips per tile (work counter, dependency
+// acquire, completion fence) than the L2-resident intermediate saves, and
+// chunks small enough for L2 lose it again to launch gaps and tails.  The
+// persistent form stays for callers that cannot allocate (a bounded static
+// scratch).
+template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int DIR, int PASS>
+__global__ void __launch_bounds__(TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>::TPB,
+                                  TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>::MIN_BLOCKS)
+k_tp_split(TwoPassParams p, int64_t b0) {
+  using TP = TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
+  using S1 = typename TP::S1;
+  using S2 = typename TP::S2;
+  using Re = typename RealOf<C>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x;
+  const C* src = static_cast<const C*>(p.src);
+  C* dst = static_cast<C*>(p.dst);
+  C* scratch = static_cast<C*>(p.scratch);
+  C v[TP::EPT];
+  if constexpr (PASS == 1) {
+    const int64_t bl = blockIdx.x / TP::TILES1;  // transform within the chunk
+    const int col0 = int(blockIdx.x % TP::TILES1) * NC1;
+    const bool active = tid < S1::TPB;
+    const int c = tid % NC1, t = tid / NC1;
+    const C* in = src + (b0 + bl) * p.idist + col0;
+    C* y = scratch + bl * TP::N;
+    col_stage<C, N1, EPT1, NC1, DIR, 1, LOAD_STREAM, OUT_SMEM_TWIDDLE, N2, 0>(
+        v, in, nullptr, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c));
+    for (int e = tid; e < N1 * NC1; e += TP::TPB) {
+      const int cc = e / N1, row = e % N1;
+      __stcg(y + int64_t(col0 + cc) * N1 + row, sh[S1::phys(row, cc)]);
+    }
+  } else {
+    const int64_t bl = blockIdx.x / TP::TILES2;
+    const int col0 = int(blockIdx.x % TP::TILES2) * NC2;
+    const bool active = tid < S2::TPB;
+    const int c = tid % NC2, t = tid / NC2;
+    const C* y = scratch + bl * TP::N + col0;
+    C* out = dst + (b0 + bl) * p.odist + col0;
+    col_stage<C, N2, EPT2, NC2, DIR, 1, LOAD_L2, OUT_COLUMNS, N1, N1>(v, y, out, sh, t, c, active,
+                                                                      static_cast<const C*>(p.tw2), Re(p.scale),
+                                                                      p.bt, 0);
+  }
+}
+
 }  // namespace gfft

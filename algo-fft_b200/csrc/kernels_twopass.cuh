@@ -13,6 +13,19 @@ cudaError_t launch_twopass(const TwoPassParams& p, int grid, cudaStream_t st) {
 }
 
 template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int DIR>
+cudaError_t launch_tp_split(const TwoPassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st) {
+  using TP = TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
+  const int64_t blocks = nb * (pass == 1 ? TP::TILES1 : TP::TILES2);
+  if (blocks <= 0) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  if (pass == 1)
+    k_tp_split<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR, 1><<<unsigned(blocks), TP::TPB, TP::SMEM, st>>>(p, b0);
+  else
+    k_tp_split<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR, 2><<<unsigned(blocks), TP::TPB, TP::SMEM, st>>>(p, b0);
+  return cudaGetLastError();
+}
+
+template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int DIR>
 TwoPassKernel make_twopass() {
   using TP = TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
   TwoPassKernel k;
@@ -26,6 +39,9 @@ TwoPassKernel make_twopass() {
   k.nc2 = NC2;
   k.func = reinterpret_cast<const void*>(&k_twopass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>);
   k.launch = &launch_twopass<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
+  k.split_func[0] = reinterpret_cast<const void*>(&k_tp_split<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR, 1>);
+  k.split_func[1] = reinterpret_cast<const void*>(&k_tp_split<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR, 2>);
+  k.split = &launch_tp_split<C, N1, EPT1, NC1, N2, EPT2, NC2, DIR>;
   return k;
 }
 
