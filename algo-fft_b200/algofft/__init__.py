@@ -9,7 +9,8 @@ from ._lib import (ErrCuda, ErrInvalidArgument, ErrInvalidLength, ErrInvalidSpec
                    ErrWisdom, GfftError, LIB_PATH, check, lib)
 from .plan import (COMPLEX64, COMPLEX128, KernelAuto, KernelBluestein, KernelDIT, KernelEightStep, KernelRecursive,
                    KernelSixStep, KernelStockham, NewPlan, NewPlan32, NewPlan64, NewPlanT, NewPlanWithOptions, Plan,
-                   PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerMeasure, PlannerPatient)
+                   PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerLearned, PlannerMeasure,
+                   PlannerPatient)
 
 from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, ConvolveReal, ConvolveRealBatch,
                        Correlate, Correlate128, CrossCorrelate, CrossCorrelate128)

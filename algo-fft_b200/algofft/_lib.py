@@ -142,6 +142,15 @@ SIGNATURES = {
     "gfft_plan_uneven_total": (I64, [P]),
     "gfft_uneven_exec": (I32, [P, I32, P, P, I32, P]),
     "gfft_uneven_exec_per_size": (I32, [P, I32, P, P, P]),
+    "gfft_mlp_sizes": (None, [ctypes.POINTER(I32), ctypes.POINTER(I32), ctypes.POINTER(I64)]),
+    "gfft_mlp_forward": (I32, [P, P, I64, P, P]),
+    "gfft_mlp_grad": (I32, [P, P, P, I64, P, P, P]),
+    "gfft_mlp_train": (I32, [P, P, P, P, P, I64, I32, I32, ctypes.c_float, ctypes.c_uint64, I64, P, P]),
+    "gfft_planner_features": (I32, [I32, I64, I64, I64, I32, CHARP, P]),
+    "gfft_planner_set_model": (I32, [P, P]),
+    "gfft_planner_load_model": (I32, [CHARP]),
+    "gfft_planner_has_model": (I32, []),
+    "gfft_planner_choose": (I32, [I32, I64, I64, I64, I32, ctypes.c_char_p, ctypes.c_size_t]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

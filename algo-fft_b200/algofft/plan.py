@@ -15,6 +15,7 @@ from ._lib import ErrNilSlice, PlanOptionsC, check, lib
 
 COMPLEX64, COMPLEX128 = 0, 1
 PlannerEstimate, PlannerMeasure, PlannerPatient, PlannerExhaustive = range(4)
+PlannerLearned = 4  # no counterpart in the reference: the learned cost model (algofft.planner)
 KernelAuto, KernelDIT, KernelStockham, KernelSixStep, KernelEightStep, KernelBluestein, KernelRecursive = range(7)
 
 

@@ -82,21 +82,10 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts = o;
-  // PlannerMeasure/Patient/Exhaustive (plan_options.go:15-33): time the
-  // compiled variants once and remember the winner in the wisdom store
-  // (internal/fft/measure.go:89-141); later plans reuse it.
-  std::string tok;
-  if (o.planner >= GFFT_PLANNER_MEASURE && o.strategy == GFFT_KERNEL_AUTO && !wisdom_lookup(n, precision, &tok) &&
-      !variant_tokens(precision, n).empty()) {
-    const int iters = o.planner == GFFT_PLANNER_MEASURE ? 10 : o.planner == GFFT_PLANNER_PATIENT ? 50 : 100;
-    std::string best, report;
-    gfft_status ts = autotune(precision, n, 0, iters, &best, &report);
-    if (ts != GFFT_OK) {
-      delete p;
-      return ts;
-    }
-  }
-  gfft_status s = core_init(&p->core, precision, n, o.device, o.strategy);
+  PlanHint hint;
+  hint.planner = o.planner;
+  hint.batch = o.batch;
+  gfft_status s = core_init(&p->core, precision, n, o.device, o.strategy, &hint);
   if (s != GFFT_OK) {
     core_free(&p->core);
     delete p;

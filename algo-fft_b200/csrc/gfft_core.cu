@@ -242,6 +242,12 @@ std::vector<std::string> variant_tokens(int prec, int64_t n) {
     if (n <= (prec == kC64 ? 16384 : 8192))
       for (const Pow2Kernel* k : pow2_variants(prec, int(n), -1)) v.push_back(pow2_token(k->n, k->ept));
     for (const TwoPassKernel* k : twopass_variants(prec, n, -1)) v.push_back(twopass_token(k));
+  } else if (n > 1 && is_smooth7(n)) {
+    // runtime-radix schedules (single CTA when it fits, two passes when n
+    // has a 7-smooth divisor >= 2 below sqrt n) against Bluestein
+    // (planner.go:50-55 picks by smoothness alone)
+    for (const std::string& t : mixed_tokens(prec, n)) v.push_back(t);
+    v.push_back("gpu-sm100-bluestein-n" + std::to_string(n));
   }
   return v;
 }
@@ -275,11 +281,19 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     const TwoPassKernel* i = find_twopass(prec, n, +1, te, e);
     if (f && i) return init_twopass(c, f, i);
   }
+  long long ln = 0, l1 = 0, l2 = 0;
+  if (std::sscanf(tok.c_str(), "gpu-sm100-mixed-n%lld", &ln) == 1 && ln == n && is_smooth7(n)) return init_generic(c);
+  if (std::sscanf(tok.c_str(), "gpu-sm100-mixed2-%lldx%lld", &l1, &l2) == 2 && l1 * l2 == n && is_smooth7(n)) {
+    gfft_status s = init_gen_twopass(c);
+    if (s == GFFT_OK && c->gn1 == l1) return s;
+    core_free(c);
+  }
+  if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1 && ln == n && n >= 2) return init_bluestein(c);
   set_error("unknown or uncompiled variant '" + tok + "' for length " + std::to_string(n));
   return GFFT_ERR_INVALID_ARGUMENT;
 }
 
-gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy) {
+gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy, const PlanHint* hint) {
   c->prec = prec;
   c->n = n;
   c->device = device;
@@ -300,6 +314,26 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
   if (strategy == GFFT_KERNEL_AUTO) {
     std::string tok;
     if (wisdom_lookup(n, prec, &tok) && core_init_variant(c, prec, n, device, tok) == GFFT_OK) return GFFT_OK;
+    core_free(c);
+    // PlannerMeasure/Patient/Exhaustive (plan_options.go:15-33): time the
+    // compiled variants once and remember the winner in the wisdom store
+    // (internal/fft/measure.go:89-141); later plans reuse it.
+    if (hint && hint->planner >= GFFT_PLANNER_MEASURE && hint->planner <= GFFT_PLANNER_EXHAUSTIVE &&
+        variant_tokens(prec, n).size() > 1) {
+      const int iters = hint->planner == GFFT_PLANNER_MEASURE ? 10 : hint->planner == GFFT_PLANNER_PATIENT ? 50 : 100;
+      std::string best, report;
+      gfft_status ts = autotune(prec, n, hint->batch > 0 ? hint->batch : 0, iters, &best, &report);
+      if (ts != GFFT_OK) return ts;
+      if (!best.empty() && core_init_variant(c, prec, n, device, best) == GFFT_OK) return GFFT_OK;
+      core_free(c);
+    }
+    if (hint && hint->planner == GFFT_PLANNER_LEARNED && learned_choose(prec, n, *hint, &tok) &&
+        core_init_variant(c, prec, n, device, tok) == GFFT_OK)
+      return GFFT_OK;
+    core_free(c);
+    c->prec = prec;
+    c->n = n;
+    c->device = device;
     clear_error();
   }
   const bool want_bluestein = strategy == GFFT_KERNEL_BLUESTEIN;

@@ -59,6 +59,8 @@ bool is_smooth7(int64_t n);
 // needs more than 1024 threads).
 bool make_gen_sched(int64_t n, GenSched* s);
 gfft_status init_generic(PlanCore* c);
+// Variant tokens of the runtime-radix schedules that can serve n.
+std::vector<std::string> mixed_tokens(int prec, int64_t n);
 gfft_status init_gen_twopass(PlanCore* c);
 gfft_status init_bluestein(PlanCore* c);
 // Column batches through the runtime column kernel (7-smooth n that fits).
@@ -74,9 +76,24 @@ gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void*
 cudaError_t ws_alloc(void** p, size_t bytes, cudaStream_t st);
 gfft_status fill_twiddles(int prec, void* dst, int64_t n, int64_t count, int64_t step, cudaStream_t st);
 
+// What plan creation knows about the calls a plan will serve; the learned
+// planner's shape features (batch 0 = unknown).
+struct PlanHint {
+  int planner = GFFT_PLANNER_ESTIMATE;
+  int64_t batch = 0;   // transforms per call
+  int64_t stride = 1;  // element stride inside one transform
+  int real = 0;        // 1: the complex child of a real transform of length 2n
+};
+
 // Chooses and prepares the schedule of a 1-D complex transform of length n:
-// a forced strategy class, else the wisdom store's variant, else defaults.
-gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy = GFFT_KERNEL_AUTO);
+// a forced strategy class, else the wisdom store's variant, else (with
+// GFFT_PLANNER_LEARNED and a model loaded) the learned cost model's pick,
+// else defaults.
+gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy = GFFT_KERNEL_AUTO,
+                      const PlanHint* hint = nullptr);
+// The learned cost model's choice among variant_tokens(prec, n) for the
+// hinted shape (false when no model is loaded or n has < 2 variants).
+bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* token);
 // Prepares the exact kernel variant named by a wisdom token.
 gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, const std::string& token);
 void core_free(PlanCore* c);

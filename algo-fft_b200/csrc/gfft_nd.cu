@@ -65,11 +65,16 @@ struct Axis {
   void* w = nullptr;   // W_n for the column kernel
 };
 
-static gfft_status axis_init(Axis* a, int prec, int64_t n, int64_t inner, int64_t outer, int device) {
+static gfft_status axis_init(Axis* a, int prec, int64_t n, int64_t inner, int64_t outer, int device, int planner,
+                             int64_t batch) {
   a->n = n;
   a->inner = inner;
   a->outer = outer;
-  gfft_status s = core_init(&a->core, prec, n, device);
+  PlanHint hint;
+  hint.planner = planner;
+  hint.batch = std::max<int64_t>(1, batch) * inner * outer;  // transforms of this axis per call
+  hint.stride = inner;
+  gfft_status s = core_init(&a->core, prec, n, device, GFFT_KERNEL_AUTO, &hint);
   if (s != GFFT_OK) return s;
   if (inner > 1 && n > 1 && column_sched(n, prec, &a->cs)) {
     s = make_twiddles(prec, n, &a->w, 0);
@@ -229,6 +234,7 @@ extern "C" gfft_status gfft_plan_nd_new(gfft_plan_nd** out, int32_t precision, i
   if (p->real) {
     gfft_plan_options ro{};
     ro.device = o.device;
+    ro.planner = o.planner;  // (ro.batch would change the real plan's buffer layout)
     s = gfft_plan_real_new(&p->rplan, precision, dims[ndims - 1], &ro);
   }
   int64_t inner = 1;
@@ -242,7 +248,7 @@ extern "C" gfft_status gfft_plan_nd_new(gfft_plan_nd** out, int32_t precision, i
         break;
       }
       p->axes.push_back(a);
-      s = axis_init(a, precision, n, inner, outer, o.device);
+      s = axis_init(a, precision, n, inner, outer, o.device, o.planner, o.batch);
     }
     inner *= n;
   }

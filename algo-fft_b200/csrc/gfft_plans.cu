@@ -168,13 +168,31 @@ static bool make_col_sched(int64_t L, size_t es, int want, GenSched* s) {
   return true;
 }
 
-gfft_status init_gen_twopass(PlanCore* c) {
-  const int64_t n = c->n;
-  const size_t es = elem_bytes(c->prec);
-  // N1: the 7-smooth divisor of n nearest below sqrt(n)
+// N1 of the runtime two-pass split: the 7-smooth divisor of n nearest below
+// sqrt(n) (1 when there is none).
+static int64_t gen_split(int64_t n) {
   int64_t n1 = 1;
   for (int64_t d = 1; d * d <= n; ++d)
     if (n % d == 0 && smooth7(d)) n1 = d;
+  return n1;
+}
+
+std::vector<std::string> mixed_tokens(int prec, int64_t n) {
+  std::vector<std::string> v;
+  const size_t es = elem_bytes(prec);
+  GenSched s, s1, s2;
+  if (make_sched(n, &s) && size_t(s.stride) * es <= size_t(kSmemBudget)) v.push_back("gpu-sm100-mixed-n" + std::to_string(n));
+  const int64_t n1 = gen_split(n), n2 = n / n1;
+  const int want = prec == kC64 ? 16 : 8;
+  if (n1 >= 2 && make_col_sched(n1, es, want, &s1) && make_col_sched(n2, es, want, &s2))
+    v.push_back("gpu-sm100-mixed2-" + std::to_string(n1) + "x" + std::to_string(n2));
+  return v;
+}
+
+gfft_status init_gen_twopass(PlanCore* c) {
+  const int64_t n = c->n;
+  const size_t es = elem_bytes(c->prec);
+  const int64_t n1 = gen_split(n);
   const int64_t n2 = n / n1;
   if (n1 < 2) return GFFT_ERR_NOT_IMPLEMENTED;
   const int want = c->prec == kC64 ? 16 : 8;

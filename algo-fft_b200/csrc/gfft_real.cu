@@ -150,7 +150,11 @@ gfft_status gfft_plan_real_new(gfft_plan_real** out, int32_t precision, int64_t 
   p->n = n;
   p->h = n / 2;
   p->opts = o;
-  gfft_status s = core_init(&p->child, precision, p->h, o.device, o.strategy);
+  PlanHint hint;
+  hint.planner = o.planner;
+  hint.batch = o.batch;
+  hint.real = 1;
+  gfft_status s = core_init(&p->child, precision, p->h, o.device, o.strategy, &hint);
   cudaError_t e = cudaSuccess;
   if (s == GFFT_OK) e = cudaMalloc(&p->wt, size_t(p->h + 1) * elem_bytes(precision));
   if (s == GFFT_OK && e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&p->flag), sizeof(unsigned));

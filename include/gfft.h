@@ -64,7 +64,10 @@ typedef enum gfft_status {
 typedef enum gfft_precision { GFFT_COMPLEX64 = 0, GFFT_COMPLEX128 = 1 } gfft_precision;
 
 /* plan_options.go:15-33 PlannerMode. */
-enum { GFFT_PLANNER_ESTIMATE = 0, GFFT_PLANNER_MEASURE = 1, GFFT_PLANNER_PATIENT = 2, GFFT_PLANNER_EXHAUSTIVE = 3 };
+enum { GFFT_PLANNER_ESTIMATE = 0, GFFT_PLANNER_MEASURE = 1, GFFT_PLANNER_PATIENT = 2, GFFT_PLANNER_EXHAUSTIVE = 3,
+       /* no counterpart in the reference: the learned cost model picks the
+        * variant when the wisdom store has none (gfft_planner_* below) */
+       GFFT_PLANNER_LEARNED = 4 };
 
 /* internal/fftypes/strategy.go:4-13 KernelStrategy. */
 enum {
@@ -317,6 +320,45 @@ GFFT_API gfft_status gfft_uneven_exec(gfft_plan_uneven* plan, int32_t direction,
  * call per transform, as a loop over Plan.Forward would do. */
 GFFT_API gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* plan, int32_t direction, void* dst,
                                                const void* src, void* stream);
+
+/* ---- learned planner (no counterpart in the reference) -------------------- */
+
+/* The cost model: an FP32 MLP, in_dim -> hidden -> hidden -> 1 with ReLU,
+ * nparams floats laid out W1[hidden][in_dim] b1 W2[hidden][hidden] b2 w3 b3
+ * (row-major).  in_dim = 16, hidden = 64. */
+GFFT_API void gfft_mlp_sizes(int32_t* in_dim, int32_t* hidden, int64_t* nparams);
+/* out[i] = model(x[i*in_dim ..]) for n samples; device pointers. */
+GFFT_API gfft_status gfft_mlp_forward(const float* params, const float* x, int64_t n, float* out, void* stream);
+/* Gradient of the mean squared error (1/n) sum (model(x_i) - y_i)^2 over
+ * samples 0..n-1 (1 <= n <= 64) with respect to every parameter, and the
+ * loss; device pointers. */
+GFFT_API gfft_status gfft_mlp_grad(const float* params, const float* x, const float* y, int64_t n, float* grad,
+                                   float* loss, void* stream);
+/* `steps` Adam steps (beta1 0.9, beta2 0.999, eps 1e-8, step counter
+ * starting after step0) on mini-batches of `batch` (<= 64) samples drawn
+ * deterministically from (seed, step) out of the n samples; params and the
+ * Adam moments adam_m, adam_v (nparams each, zero at the start) are updated
+ * in place; *loss (device) = mean mini-batch loss of these steps. */
+GFFT_API gfft_status gfft_mlp_train(float* params, float* adam_m, float* adam_v, const float* x, const float* y,
+                                    int64_t n, int32_t steps, int32_t batch, float lr, uint64_t seed, int64_t step0,
+                                    float* loss, void* stream);
+/* Raw features (in_dim floats, host) of the variant `token` for a shape:
+ * complex length n (the complex child length for real = 1), batch
+ * transforms per call (<= 0: unknown, taken as 128 MB of data), element
+ * stride.  Host-only. */
+GFFT_API gfft_status gfft_planner_features(int32_t precision, int64_t n, int64_t batch, int64_t stride, int32_t real,
+                                           const char* token, float* out);
+/* Installs the model used by GFFT_PLANNER_LEARNED (host arrays: nparams
+ * parameters; norm = feature means[in_dim], deviations[in_dim], target mean,
+ * target deviation), or unloads it (params NULL).  Without a call, the file
+ * wisdom/planner_b200.bin next to the library is loaded on first use. */
+GFFT_API gfft_status gfft_planner_set_model(const float* params, const float* norm);
+GFFT_API gfft_status gfft_planner_load_model(const char* path);
+GFFT_API int32_t gfft_planner_has_model(void);
+/* The model's pick among gfft_plan_variants(n) for a shape (one inference
+ * launch on the current device). */
+GFFT_API gfft_status gfft_planner_choose(int32_t precision, int64_t n, int64_t batch, int64_t stride, int32_t real,
+                                         char* token, size_t cap);
 
 /* ---- errors -------------------------------------------------------------- */
 

@@ -61,4 +61,6 @@ def test_variants_listed_without_device():
     assert "gpu-sm100-p2-n1024-e32" in v and "gpu-sm100-tp-32x32-t8192-e16" not in v
     v = algofft.Variants(1 << 20)
     assert any(t.startswith("gpu-sm100-tp-1024x1024-") for t in v)
-    assert algofft.Variants(1000) == []
+    # 7-smooth lengths: runtime-radix schedules against Bluestein
+    assert algofft.Variants(1000) == ["gpu-sm100-mixed-n1000", "gpu-sm100-mixed2-25x40", "gpu-sm100-bluestein-n1000"]
+    assert algofft.Variants(1009) == []  # a prime: Bluestein is the only schedule
