@@ -1,13 +1,19 @@
-"""Benchmark of the batched complex64 C2C path (Plan.ForwardBatch) on B200.
+"""Benchmark of the batched C2C path (Plan.ForwardBatch) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step"): one ForwardBatch per length of the power-of-two sweep,
-each over a 1 GiB batch of complex64 (count = 2^27 / N transforms), inputs
-i.i.d. N(0,1) from a fixed seed, resident in HBM.  Every batch is larger than
-the 126 MB L2, so no flush is needed between steps.  The metric is
-algorithmic HBM bandwidth: 16*N bytes per transform (one read and one write
-of 8*N bytes) divided by device time.
+Workload (one "step"): one ForwardBatch per length of the power-of-two sweep
+N = 2^4..2^24, each over a 1 GiB batch of complex64 (count = 2^27 / N
+transforms), inputs i.i.d. N(0,1) from a fixed seed, resident in HBM.  Every
+batch is larger than the 126 MB L2, so no flush is needed between steps.  The
+metric is algorithmic HBM bandwidth: 16*N bytes per transform (one read and
+one write of 8*N bytes) divided by device time; `value` aggregates the sweep.
+
+Measured beside it, outside the timed region of `value` (under "extras"):
+the complex128 sweep (1 GiB batches), R2C/C2R float32 N=4096 x 65536, the
+uneven-length batch (20,000 transforms: 50% 2^6..2^16, 30% 7-smooth <= 65536,
+20% primes 1009..65521) against the plain per-size path, and ConvolveReal of
+64 x 2^20 reals with a 4097-tap kernel.
 
 Multi-GPU (torchrun): batches shard across ranks (each rank runs the same
 per-rank workload, no collective on the data path, weak scaling); time is the
@@ -32,8 +38,21 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "algo-fft_b200"))
 
 BUF_BYTES = 1 << 30                      # one 1 GiB batch per length
-SWEEP = [2 ** k for k in range(10, 25)]
-WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^10..2^24, 1 GiB batch per N"
+SWEEP = [2 ** k for k in range(4, 25)]
+WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^4..2^24, 1 GiB batch per N"
+
+# DRAM bytes per transform (read + write) of the two-pass kernels, from
+# ncu captures of small batches (profiles/k_tp_split_twopass.md); used to
+# scale `roofline.traffic` to a full launch.
+TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6}
+
+
+def launches_of(algorithm: str, count: int, n: int, es: int) -> int:
+    """Kernel launches of one ForwardBatch of this plan."""
+    if "-tp-" in algorithm:
+        chunk = max(1, min(count, (1 << 30) // (n * es)))
+        return 2 * ((count + chunk - 1) // chunk)
+    return 1
 
 
 def bytes_per_transform(n: int) -> int:
@@ -160,6 +179,108 @@ def run_reference(args):
     return 0
 
 
+def _median_ms(fn, stream, iters: int, warm: int = 1) -> float:
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(iters):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def extras(dev, stream, iters: int) -> dict:
+    """Device-timed figures of the other measured workloads (median of
+    `iters` runs after one warm-up), each with its own accuracy check."""
+    import numpy as np
+    import torch
+    import algofft
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    out = {}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(77)
+
+    # complex128 sweep, 1 GiB batches
+    x = torch.randn(BUF_BYTES // 8, generator=gen, device=dev, dtype=torch.float64).view(torch.complex128)
+    y = torch.empty_like(x)
+    c128 = {}
+    for n in SWEEP:
+        count = BUF_BYTES // (16 * n)
+        with algofft.NewPlan64(n) as p:
+            ms = _median_ms(lambda: p.ForwardBatch(y, x, count), stream, iters)
+            c128[str(n)] = 32 * n * count / (ms / 1e3) / 1e9
+    ref = oracle.batch(x[:4096].cpu().numpy(), 4096)
+    with algofft.NewPlan64(4096) as p:
+        p.ForwardBatch(y, x, 1)
+    err128 = float(np.linalg.norm(y[:4096].cpu().numpy() - ref) / np.linalg.norm(ref))
+    out["c128_sweep"] = {"unit": "GB/s", "bytes_per_transform": "32*N", "per_size_gbs": c128,
+                         "rel_l2_vs_fp64_n4096": err128}
+    del x, y
+
+    # R2C / C2R float32, N = 4096, batch 65536
+    n, batch = 4096, 65536
+    xr = torch.rand(n * batch, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
+    X = torch.empty(batch * (n // 2 + 1), dtype=torch.complex64, device=dev)
+    back = torch.empty_like(xr)
+    with algofft.NewPlanRealWithOptions(n, algofft.PlanOptions(Batch=batch)) as p:
+        f_ms = _median_ms(lambda: p.Forward(X, xr), stream, iters)
+        i_ms = _median_ms(lambda: p.Inverse(back, X), stream, iters)
+    rb = 4 * n + 8 * (n // 2 + 1)
+    spec = np.fft.rfft(xr[:n].cpu().numpy().astype(np.float64))
+    err = float(np.linalg.norm(X[:n // 2 + 1].cpu().numpy() - spec) / np.linalg.norm(spec))
+    out["real_4096x65536"] = {"unit": "GB/s", "bytes_per_transform": rb,
+                              "r2c_gbs": rb * batch / (f_ms / 1e3) / 1e9, "c2r_gbs": rb * batch / (i_ms / 1e3) / 1e9,
+                              "rel_l2_vs_fp64": err}
+    del xr, X, back
+
+    # uneven-length batch: one plan, graph replay, against the per-size path
+    L = algofft.uneven_lengths(20000, seed=0)
+    with algofft.PlanUneven(L) as p:
+        tot = p.Total()
+        xu = torch.randn(2 * tot, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+        yu = torch.empty_like(xu)
+        g_ms = _median_ms(lambda: p.Forward(yu, xu), stream, iters)
+        ps_ms = _median_ms(lambda: p.ForwardPerSize(yu, xu), stream, 2)
+        p.Forward(yu, xu)
+        torch.cuda.synchronize()
+        xh = xu[:int(L[:40].sum())].cpu().numpy().astype(np.complex128)
+        yh = yu[:int(L[:40].sum())].cpu().numpy()
+    errs, off = [], 0
+    for n in L[:40]:
+        r = np.fft.fft(xh[off:off + n])
+        errs.append(float(np.linalg.norm(yh[off:off + n] - r) / np.linalg.norm(r)))
+        off += n
+    out["uneven_20000"] = {"transforms": 20000, "elements": int(tot),
+                           "transforms_per_s": 20000 / (g_ms / 1e3),
+                           "per_size_transforms_per_s": 20000 / (ps_ms / 1e3),
+                           "speedup_vs_per_size": ps_ms / g_ms, "ms": g_ms, "per_size_ms": ps_ms,
+                           "gbs_user_bytes": 16 * tot / (g_ms / 1e3) / 1e9,
+                           "max_rel_l2_first_40": max(errs)}
+    del xu, yu
+
+    # ConvolveReal: 64 signals of 2^20 reals with a 4097-tap kernel
+    cnt, na, nb = 64, 1 << 20, 4097
+    a = torch.rand(cnt * na, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
+    k = torch.rand(nb, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
+    d = torch.empty(cnt * (na + nb - 1), dtype=torch.float32, device=dev)
+    c_ms = _median_ms(lambda: algofft.ConvolveRealBatch(d, a, na, cnt, k), stream, iters)
+    cb = 4 * na + 4 * nb + 4 * (na + nb - 1)
+    av, kv, dv = a[:na].cpu().numpy().astype(np.float64), k.cpu().numpy().astype(np.float64), d[:na + nb - 1].cpu().numpy()
+    ref = np.fft.irfft(np.fft.rfft(av, 1 << 21) * np.fft.rfft(kv, 1 << 21), 1 << 21)[:na + nb - 1]
+    out["convolve_real_64x2^20_k4097"] = {"unit": "GB/s", "bytes_per_signal": cb,
+                                          "gbs": cnt * cb / (c_ms / 1e3) / 1e9, "ms": c_ms,
+                                          "rel_l2_vs_fp64": float(np.linalg.norm(dv - ref) / np.linalg.norm(ref))}
+    return out
+
+
 def main():
     global SWEEP, BUF_BYTES
     ap = argparse.ArgumentParser()
@@ -169,6 +290,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-slice leg (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the c128/real/uneven/convolve figures")
     ap.add_argument("--sizes", default="", help="comma-separated subset of lengths (profiling runs)")
     ap.add_argument("--batch-mib", type=int, default=BUF_BYTES >> 20, help="batch bytes per length in MiB")
     args = ap.parse_args()
@@ -219,41 +341,44 @@ def main():
         pg.barrier()
 
     per_size_ms = {n: 0.0 for n in SWEEP}
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
     mark = clk.mark()
-    if True:
+    torch.cuda.synchronize()
+    for s_ in range(args.steps):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in SWEEP]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        step(evs)
         torch.cuda.synchronize()
-        start.record(stream)
-        for s in range(args.steps):
-            evs = [torch.cuda.Event(enable_timing=True) for _ in SWEEP]
-            t0 = torch.cuda.Event(enable_timing=True)
-            t0.record(stream)
-            step(evs)
-            torch.cuda.synchronize()
-            prev = t0
-            for i, n in enumerate(SWEEP):
-                per_size_ms[n] += prev.elapsed_time(evs[i])
-                prev = evs[i]
-        end.record(stream)
-        torch.cuda.synchronize()
+        prev = t0
+        for i, n in enumerate(SWEEP):
+            per_size_ms[n] += prev.elapsed_time(evs[i])
+            prev = evs[i]
+    torch.cuda.synchronize()
     time.sleep(0.3)
-    clk.__exit__()
-    total_ms = start.elapsed_time(end)
-    dev_ms = sum(per_size_ms.values())  # kernels only (host gaps between steps excluded)
+    clocks = clk.summary(mark)
+    dev_ms = sum(per_size_ms.values())  # device time of the K steps (events back to back)
     t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
     if pg:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
     dev_ms = float(t.item())
     bytes_step = sum(bytes_per_transform(n) * bufs[n][2] for n in SWEEP)
     value = world * bytes_step * args.steps / (dev_ms / 1e3) / 1e9
+    launches_step = sum(launches_of(plans[n].Algorithm(), bufs[n][2], n, 8) for n in SWEEP)
 
     # dominant kernel: the length with the largest share of device time
     dom = max(SWEEP, key=lambda n: per_size_ms[n])
-    dom_ms = per_size_ms[dom] / args.steps
-    dom_bytes = bytes_per_transform(dom) * bufs[dom][2]
+    dom_alg = plans[dom].Algorithm()
+    dom_launches = launches_of(dom_alg, bufs[dom][2], dom, 8)
+    dom_ms = per_size_ms[dom] / args.steps / dom_launches  # average launch duration
+    dom_bytes = bytes_per_transform(dom) * bufs[dom][2] / dom_launches  # algorithmic bytes per launch
     peak, peak_kind = peak_hbm()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    if "-tp-" in dom_alg:
+        kname = f"k_tp_split (two-pass, pass 1 and pass 2 alternate; N={dom}, {dom_alg})"
+    else:
+        kname = f"k_pow2 (single pass; N={dom}, {dom_alg})"
+    traffic = TRAFFIC_PER_TRANSFORM.get(dom_alg)
+    traffic = traffic * bufs[dom][2] / dom_launches if traffic else None
 
     # correctness at the stated error on the first transforms of each batch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -263,33 +388,45 @@ def main():
         x, y, count = bufs[n]
         plans[n].ForwardBatch(y, x, count)
         torch.cuda.synchronize()
-        xs = x[: n].cpu().numpy().astype(np.complex128)
-        ys = y[: n].cpu().numpy().astype(np.complex128)
+        k = max(1, min(count, 4096 // n))
+        xs = x[: k * n].cpu().numpy().astype(np.complex128)
+        ys = y[: k * n].cpu().numpy().astype(np.complex128)
         ref = oracle.batch(xs, n)
         errs[n] = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
     # end to end: the same sweep through the host-slice API (pinned host
-    # buffers, H2D + transform + D2H inside the timed region, every step)
+    # buffers; copies in, transforms and copies out inside the timed region,
+    # every step), timed on the host around whole calls
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
-    hx_t = torch.empty(xin.numel(), dtype=torch.complex64, pin_memory=True)
-    hx_t.copy_(xin)
-    hy_t = torch.empty_like(hx_t, pin_memory=True)
-    host = {n: (hx_t.numpy(), hy_t.numpy(), bufs[n][2]) for n in SWEEP}
-    for n in SWEEP if e2e_steps else []:  # warm the staging pool
-        hx, hy, count = host[n]
-        plans[n].ForwardBatch(hy, hx, count)
-    if pg:
-        pg.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        for n in SWEEP:
+    e2e_val = None
+    if e2e_steps:
+        hx_t = torch.empty(xin.numel(), dtype=torch.complex64, pin_memory=True)
+        hx_t.copy_(xin)
+        hy_t = torch.empty_like(hx_t, pin_memory=True)
+        host = {n: (hx_t.numpy(), hy_t.numpy(), bufs[n][2]) for n in SWEEP}
+        for n in SWEEP:  # warm the staging pool
             hx, hy, count = host[n]
             plans[n].ForwardBatch(hy, hx, count)
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-    if pg:
-        pg.all_reduce(te, op=pg.ReduceOp.MAX)
-    e2e_val = world * bytes_step * e2e_steps / max(float(te.item()), 1e-9) / 1e9
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for n in SWEEP:
+                hx, hy, count = host[n]
+                plans[n].ForwardBatch(hy, hx, count)
+        e2e_s = time.perf_counter() - t0
+        te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        if pg:
+            pg.all_reduce(te, op=pg.ReduceOp.MAX)
+        e2e_val = world * bytes_step * e2e_steps / max(float(te.item()), 1e-9) / 1e9
+        del hx_t, hy_t, host
+
+    ext = None
+    if rank == 0 and not args.no_extras and world == 1:
+        del xin, yout
+        bufs = {n: (None, None, b[2]) for n, b in bufs.items()}
+        torch.cuda.empty_cache()
+        ext = extras(dev, stream, max(3, min(args.steps, 10)))
 
     if rank == 0:
         line = {
@@ -300,22 +437,27 @@ def main():
             "config": {"workload": WORKLOAD, "sizes": SWEEP, "batch_bytes": BUF_BYTES,
                        "l2": "inputs (1 GiB per batch) larger than the 126 MB L2; no flush",
                        "parallelism": f"batch sharding x{world} (no collective)"},
+            "frac_of_peak": value / peak,
             "per_size_gbs": {str(n): bytes_per_transform(n) * bufs[n][2] * args.steps / (per_size_ms[n] / 1e3) / 1e9
                              for n in SWEEP},
             "rel_l2_vs_fp64": {str(n): errs[n] for n in SWEEP},
-            "roofline": {"bound": "hbm", "kernel": f"k_pow2 N={dom} ({plans[dom].Algorithm()})",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": None,
-                         "algorithmic_bytes_per_launch": dom_bytes},
-            "clocks": clk.summary(mark),
+            "tolerance": "rel L2 <= 1e-6*log2(N) (complex64)",
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes, "launches_per_step": dom_launches},
+            "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": bytes_step // 2,
                     "d2h_bytes_per_step": bytes_step // 2, "steps": e2e_steps,
-                    "path": "Plan.ForwardBatch on pinned host slices (gfft_forward_batch_host)"},
-            "gpu_launches": args.steps * len(SWEEP),
+                    "path": "Plan.ForwardBatch on pinned host slices (gfft_forward_batch_host: 64 MB chunks, "
+                            "copy in / transform / copy out pipelined over two streams)"},
+            "gpu_launches": args.steps * launches_step,
         }
+        if ext is not None:
+            line["extras"] = ext
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line))
+    clk.__exit__()
     for p in plans.values():
         p.Close()
     if pg:
