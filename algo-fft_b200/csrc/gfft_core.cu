@@ -289,6 +289,7 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     core_free(c);
   }
   if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1 && ln == n && n >= 2) return init_bluestein(c);
+  if (std::sscanf(tok.c_str(), "gpu-sm100-tc16-n%lld", &ln) == 1 && ln == n) return init_tc(c);
   set_error("unknown or uncompiled variant '" + tok + "' for length " + std::to_string(n));
   return GFFT_ERR_INVALID_ARGUMENT;
 }
@@ -441,6 +442,8 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
     case Algo::GenTwoPass:
     case Algo::Bluestein:
       return exec_runtime_plan(c, dir, dst, src, count, idist, odist, st);
+    case Algo::TensorCore:
+      return exec_tc(c, dir, dst, src, count, idist, odist, st);
     case Algo::Pow2Smem: {
       const Pow2Kernel* k = c->k[dir < 0 ? 0 : 1];
       const double scale = dir < 0 ? 1.0 : 1.0 / double(c->n);

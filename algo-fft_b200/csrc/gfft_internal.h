@@ -21,7 +21,7 @@ gfft_status cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::gfft::cuda_status(e_, #call); \
   } while (0)
 
-enum class Algo { Trivial, Pow2Smem, TwoPass, Generic, GenTwoPass, Bluestein };
+enum class Algo { Trivial, Pow2Smem, TwoPass, Generic, GenTwoPass, Bluestein, TensorCore };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
 // FP64 and rounded to the element type (internal/math/twiddle.go:8-21).
@@ -63,6 +63,11 @@ gfft_status init_generic(PlanCore* c);
 std::vector<std::string> mixed_tokens(int prec, int64_t n);
 gfft_status init_gen_twopass(PlanCore* c);
 gfft_status init_bluestein(PlanCore* c);
+// Tensor-core split-fp16 radix-16 form (complex64, n = 16^s, 16 <= n <= 2^24).
+bool tc_supported(int64_t n);
+gfft_status init_tc(PlanCore* c);
+gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
+                    int64_t odist, cudaStream_t st);
 // Column batches through the runtime column kernel (7-smooth n that fits).
 bool column_sched(int64_t n, int prec, GenSched* s);
 gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const void* src, int64_t count,

@@ -68,6 +68,15 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
+def tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms while timing."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -265,6 +274,48 @@ def extras(dev, stream, iters: int) -> dict:
                            "gbs_user_bytes": 16 * tot / (g_ms / 1e3) / 1e9,
                            "max_rel_l2_first_40": max(errs)}
     del xu, yu
+
+    # precision form: tensor-core split-fp16 radix-16 stages against the FP32
+    # CUDA-core path, complex64, batches of 2 GiB, two input sets
+    tcr = {}
+    peak_tf = tensor_peak()
+    for n in (256, 4096, 65536, 1 << 20):
+        count = (1 << 31) // (8 * n)
+        stages = int(round(np.log(n) / np.log(16)))
+        xt = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+        yt = torch.empty_like(xt)
+        row = {"count": count}
+        for name, var in (("tensor_core", f"gpu-sm100-tc16-n{n}"), ("fp32_cuda_core", None)):
+            with (algofft.Plan(n, algofft.COMPLEX64, variant=var) if var else algofft.NewPlan(n)) as p:
+                ms = _median_ms(lambda: p.ForwardBatch(yt, xt, count), stream, iters)
+                errs = {}
+                for kind in ("normal", "loguniform"):
+                    k = max(1, min(count, (1 << 20) // n))
+                    rng = np.random.default_rng(n)
+                    if kind == "normal":
+                        xs = (rng.standard_normal(k * n) + 1j * rng.standard_normal(k * n)).astype(np.complex64)
+                    else:
+                        xs = (10 ** rng.uniform(-4, 4, k * n) * np.exp(1j * rng.uniform(0, 2 * np.pi, k * n))
+                              ).astype(np.complex64)
+                    xd = torch.from_numpy(xs).to(dev)
+                    yd = torch.empty_like(xd)
+                    p.ForwardBatch(yd, xd, k)
+                    torch.cuda.synchronize()
+                    ref = np.fft.fft(xs.reshape(k, n).astype(np.complex128), axis=1).ravel()
+                    got = yd.cpu().numpy().astype(np.complex128)
+                    errs[kind] = {"rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                                  "max_err_rel_to_max": float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))}
+            ent = {"ms": ms, "gbs": 16 * n * count / (ms / 1e3) / 1e9, "errors": errs}
+            if var:
+                flops = 6144.0 * stages * (n // 16) * count  # 3 split products x 2*32*32 per butterfly-stage
+                ent["tensor_tflops"] = flops / (ms / 1e3) / 1e12
+                ent["tensor_frac_of_peak"] = ent["tensor_tflops"] / peak_tf
+            row[name] = ent
+        tcr[str(n)] = row
+        del xt, yt
+    out["precision_form_c64_2GiB"] = {"tolerance": "rel L2 <= 1e-6*log2(N)", "bf16_peak_tflops": peak_tf,
+                                      "flops_convention": "GEMM-equivalent: 3 split products x 2*32*32 per "
+                                                          "radix-16 butterfly per stage", "per_size": tcr}
 
     # ConvolveReal: 64 signals of 2^20 reals with a 4097-tap kernel
     cnt, na, nb = 64, 1 << 20, 4097
