@@ -132,6 +132,25 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def shard(count: int, rank: int, world: int) -> tuple[int, int]:
+    """Transforms [lo, hi) of a batch of `count` that rank `rank` of `world`
+    runs when a fixed batch is split (the batched path has no exchange
+    step: every transform is independent, so any split is exact)."""
+    lo = count * rank // world
+    return lo, count * (rank + 1) // world
+
+
+def max_over_ranks(value: float, pg=None, device=None) -> float:
+    """Max of a per-rank measurement over all ranks (identity without a
+    process group): the job's time is its slowest rank's."""
+    if pg is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -407,11 +426,7 @@ def main():
     torch.cuda.synchronize()
     time.sleep(0.3)
     clocks = clk.summary(mark)
-    dev_ms = sum(per_size_ms.values())  # device time of the K steps (events back to back)
-    t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    dev_ms = float(t.item())
+    dev_ms = max_over_ranks(sum(per_size_ms.values()), pg, dev)  # device time of the K steps
     bytes_step = sum(bytes_per_transform(n) * bufs[n][2] for n in SWEEP)
     value = world * bytes_step * args.steps / (dev_ms / 1e3) / 1e9
     launches_step = sum(launches_of(plans[n].Algorithm(), bufs[n][2], n, 8) for n in SWEEP)
@@ -465,11 +480,8 @@ def main():
             for n in SWEEP:
                 hx, hy, count = host[n]
                 plans[n].ForwardBatch(hy, hx, count)
-        e2e_s = time.perf_counter() - t0
-        te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        if pg:
-            pg.all_reduce(te, op=pg.ReduceOp.MAX)
-        e2e_val = world * bytes_step * e2e_steps / max(float(te.item()), 1e-9) / 1e9
+        e2e_s = max_over_ranks(time.perf_counter() - t0, pg, dev)
+        e2e_val = world * bytes_step * e2e_steps / max(e2e_s, 1e-9) / 1e9
         del hx_t, hy_t, host
 
     ext = None
