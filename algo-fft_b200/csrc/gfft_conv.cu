@@ -4,7 +4,10 @@
 //
 // Same algorithm as the reference: complex convolution at the exact length
 // len(a)+len(b)-1 (so it may run Bluestein), real convolution at
-// NextPow2(len(a)+len(b)-1) (at least 2).  The two forward transforms run
+// NextPow2(len(a)+len(b)-1) (at least 2) -- except for long real signals
+// with a short kernel (len(b) - 1 <= L/4 for an L <= 2^15 block and more
+// than two blocks of output), which run overlap-save (k_conv_os): the same
+// linear convolution from single-CTA transforms of 2^12..2^15 points.  The two forward transforms run
 // as one batch of two, the pointwise product is one elementwise kernel
 // (internal/fft/complex_mul.go:23), the inverse writes straight into a
 // padded buffer whose head is the result.  Plans come from a process-wide
@@ -14,6 +17,7 @@
 #include <mutex>
 #include <tuple>
 #include "gfft_internal.h"
+#include "gfft_real.cuh"
 
 namespace gfft {
 
@@ -95,6 +99,154 @@ __global__ void k_take_rows(T* dst, int64_t ddist, const T* src, int64_t sdist, 
   }
 }
 
+// ---- overlap-save for long real signals ------------------------------------
+//
+// Block j of a signal produces outputs [j B, j B + B) from the input window
+// [j B - (nb - 1), j B - (nb - 1) + L), B = L - (nb - 1): a real transform of
+// length L = 2H of the window, the product with the kernel's spectrum (L/2+1
+// bins, shared by every block and signal, L2-resident), and the inverse
+// real transform, whose samples from nb - 1 on are the linear convolution.
+// One CTA slot per block does all of it in shared memory: the window loads
+// straight into the first Stockham stage, the R2C recombination, the
+// product and the C2R packing happen pairwise (k, H - k) between the two
+// half-length transforms, and the last stage stores the B new samples.
+// HBM sees L/B reads and one write per output sample.
+
+template <typename R>
+struct WindowLoad {
+  static constexpr bool kShared = false;
+  const R* x;
+  int64_t pos0, len;
+  bool valid;
+  __device__ __forceinline__ Cx<R> operator()(int e) const {
+    const int64_t p = pos0 + 2 * int64_t(e);
+    Cx<R> v{R(0), R(0)};
+    if (valid) {
+      if (p >= 0 && p < len) v.x = x[p];
+      if (p + 1 >= 0 && p + 1 < len) v.y = x[p + 1];
+    }
+    return v;
+  }
+};
+
+template <typename C, int N, int EPT>
+struct SharedLoad {
+  static constexpr bool kShared = true;
+  const C* sh;
+  __device__ __forceinline__ C operator()(int e) const { return sh[Pow2Shape<N, EPT, sizeof(C)>::pad(e)]; }
+};
+
+template <typename R>
+struct WindowStore {
+  static constexpr bool kShared = false;
+  R* y;
+  int64_t pos0, len;  // output index of window sample 0, outputs per signal
+  int skip;           // the first nb - 1 window samples are wrapped: not outputs
+  R scale;
+  bool valid;
+  __device__ __forceinline__ void operator()(int e, Cx<R> v) const {
+    if (!valid) return;
+    const int w = 2 * e;
+    const int64_t o = pos0 + w;
+    if (w >= skip && o < len) y[o] = v.x * scale;
+    if (w + 1 >= skip && o + 1 < len) y[o + 1] = v.y * scale;
+  }
+};
+
+template <typename C, int H, int EPT>
+__global__ void __launch_bounds__(Pow2Shape<H, EPT, sizeof(C)>::TPB)
+k_conv_os(const typename RealOf<C>::type* a, typename RealOf<C>::type* dst, int64_t na, int64_t a_dist,
+          int64_t dst_dist, int64_t nout, int64_t nblk, int64_t total, int nb, const C* __restrict__ tw,
+          const C* __restrict__ wt, const C* __restrict__ hs) {
+  using R = typename RealOf<C>::type;
+  using S = Pow2Shape<H, EPT, sizeof(C)>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw) + (threadIdx.x / S::T) * S::STRIDE;
+  const int t = threadIdx.x % S::T;
+  const int64_t g = int64_t(blockIdx.x) * S::B + threadIdx.x / S::T;  // block over all signals
+  const bool valid = g < total;
+  const int64_t sig = valid ? g / nblk : 0, j = valid ? g % nblk : 0;
+  const int64_t B = 2 * int64_t(H) - (nb - 1);
+  const int64_t pos0 = j * B - (nb - 1);
+  WindowLoad<R> ld{a + sig * a_dist, pos0, na, valid};
+  PaddedStore<C, H, EPT> st{sh};
+  pow2_fft<C, H, EPT, -1>(sh, t, tw, ld, st);
+  xsync<S::T>();
+  // Z (half-length spectrum) -> X (real spectrum) -> X * Hs -> packed Z'
+  const C z0 = sh[0];
+  const C x0 = cmul(C{z0.x + z0.y, R(0)}, __ldg(hs));
+  const C xh = cmul(C{z0.x - z0.y, R(0)}, __ldg(hs + H));
+  C zp[EPT];
+#pragma unroll
+  for (int i = 0; i < EPT; ++i) {
+    const int k = t + i * S::T;
+    const C zk = sh[S::pad(k)], zhk = sh[S::pad(k == 0 ? 0 : H - k)];
+    const C xk = k == 0 ? x0 : cmul(r2c_bin(z0, zk, zhk, __ldg(wt + k), k, H), __ldg(hs + k));
+    const C xhk = k == 0 ? xh : cmul(r2c_bin(z0, zhk, zk, __ldg(wt + H - k), H - k, H), __ldg(hs + H - k));
+    zp[i] = c2r_packed(xk, xhk, x0, xh, __ldg(wt + k), k);
+  }
+  xsync<S::T>();
+#pragma unroll
+  for (int i = 0; i < EPT; ++i) sh[S::pad(t + i * S::T)] = zp[i];
+  xsync<S::T>();
+  SharedLoad<C, H, EPT> ld2{sh};
+  WindowStore<R> st2{dst + sig * dst_dist, j * B - (nb - 1), nout, nb - 1, R(1.0 / double(H)), valid};
+  pow2_fft<C, H, EPT, +1>(sh, t, tw, ld2, st2);
+}
+
+template <typename C, int H, int EPT>
+cudaError_t launch_conv_os(const void* a, void* dst, int64_t na, int64_t a_dist, int64_t dst_dist, int64_t nout,
+                           int64_t nblk, int64_t count, int nb, const void* tw, const void* wt, const void* hs,
+                           cudaStream_t st) {
+  using S = Pow2Shape<H, EPT, sizeof(C)>;
+  static const cudaError_t attr =
+      S::SMEM > 48 * 1024
+          ? cudaFuncSetAttribute(&k_conv_os<C, H, EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM)
+          : cudaSuccess;
+  if (attr != cudaSuccess) return attr;
+  using R = typename RealOf<C>::type;
+  const int64_t total = count * nblk;
+  k_conv_os<C, H, EPT><<<unsigned((total + S::B - 1) / S::B), S::TPB, S::SMEM, st>>>(
+      static_cast<const R*>(a), static_cast<R*>(dst), na, a_dist, dst_dist, nout, nblk, total, nb,
+      static_cast<const C*>(tw), static_cast<const C*>(wt), static_cast<const C*>(hs));
+  return cudaGetLastError();
+}
+
+// FFT length of the overlap-save blocks: the smallest power of two with at
+// most a quarter of each window wrapped (L >= 4 (nb - 1)), at least 4096, at
+// most what one CTA transforms (2 x 16384 complex64, 2 x 8192 complex128);
+// 0 = use one transform of the whole signal (short signals, long kernels).
+template <typename R>
+int64_t os_length(int64_t na, int64_t nb) {
+  const int64_t lmax = sizeof(R) == 4 ? 32768 : 16384;
+  int64_t L = 4096;
+  while (L < 4 * (nb - 1)) L <<= 1;
+  if (L > lmax || na + nb - 1 <= 2 * L) return 0;
+  return L;
+}
+
+template <typename R>
+cudaError_t dispatch_conv_os(int64_t L, const R* a, R* dst, int64_t na, int64_t a_dist, int64_t dst_dist,
+                             int64_t nout, int64_t nblk, int64_t count, int nb, const void* tw, const void* wt,
+                             const void* hs, cudaStream_t st) {
+  using C = Cx<R>;
+  if constexpr (sizeof(R) == 4) {
+    switch (L) {
+      case 4096: return launch_conv_os<C, 2048, 16>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+      case 8192: return launch_conv_os<C, 4096, 16>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+      case 16384: return launch_conv_os<C, 8192, 32>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+      case 32768: return launch_conv_os<C, 16384, 32>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+    }
+  } else {
+    switch (L) {
+      case 4096: return launch_conv_os<C, 2048, 16>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+      case 8192: return launch_conv_os<C, 4096, 16>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+      case 16384: return launch_conv_os<C, 8192, 16>(a, dst, na, a_dist, dst_dist, nout, nblk, count, nb, tw, wt, hs, st);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace
 
 // Complex: dst[0, L) = IFFT_L(FFT_L(a) * FFT_L(b)), L = na + nb - 1.
@@ -131,6 +283,30 @@ static gfft_status convolve_real_dev(int prec, R* dst, int64_t dst_dist, const R
                                      int64_t count, const R* b, int64_t nb, cudaStream_t st) {
   using C = Cx<R>;
   const int64_t L = na + nb - 1;
+  // long signals: overlap-save blocks (same linear convolution, transforms
+  // of 2^12..2^15 points instead of one of NextPow2(na + nb - 1))
+  if (const int64_t Lb = os_length<R>(na, nb)) {
+    gfft_plan_real* bp = nullptr;
+    gfft_status s = cached_real_plan(prec, Lb, &bp);
+    if (s != GFFT_OK) return s;
+    if (bp->child.algo == Algo::Pow2Smem) {
+      const int64_t hb = Lb / 2 + 1;
+      R* kpad = nullptr;
+      GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&kpad), size_t(Lb) * sizeof(R) + size_t(hb) * sizeof(C), st));
+      C* hs = reinterpret_cast<C*>(kpad + Lb);
+      k_pad<R><<<grid1(Lb), 256, 0, st>>>(kpad, Lb, b, nb, 0, 1, false);
+      cudaError_t e = cudaGetLastError();
+      if (e == cudaSuccess) s = real_forward(bp, 0, hs, kpad, 1, Lb, hb, st);
+      if (e == cudaSuccess && s == GFFT_OK) {
+        const int64_t B = Lb - (nb - 1), nblk = (L + B - 1) / B;
+        e = dispatch_conv_os<R>(Lb, a, dst, na, a_dist, count == 1 ? L : dst_dist, L, nblk, count, int(nb),
+                                bp->child.tw, bp->wt, hs, st);
+      }
+      cudaFreeAsync(kpad, st);
+      if (e != cudaSuccess) return cuda_status(e, "k_conv_os");
+      return s;
+    }
+  }
   int64_t F = 2;
   while (F < L) F <<= 1;  // convolve_real.go:23-28
   const int64_t h1 = F / 2 + 1;

@@ -102,6 +102,44 @@ def test_convolve_real_batch_shared_kernel():
         assert (torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref)).item() <= TOL
 
 
+@pytest.mark.parametrize("na,nb", [(20000, 1), (50001, 2049), (100000, 8193), (12289, 2), (300000, 4097)])
+def test_convolve_real_overlap_save_lengths(na, nb):
+    # long signals with short kernels run overlap-save blocks of 2^12..2^15
+    # points; the result is the same linear convolution
+    rng = np.random.default_rng(na + nb)
+    a = rng.uniform(-1, 1, na).astype(np.float32)
+    b = rng.uniform(-1, 1, nb).astype(np.float32)
+    got = np.empty(na + nb - 1, np.float32)
+    algofft.ConvolveReal(got, a, b)
+    F = 1 << int(np.ceil(np.log2(na + nb - 1)))
+    ref = np.fft.irfft(np.fft.rfft(a.astype(np.float64), F) * np.fft.rfft(b.astype(np.float64), F), F)[:na + nb - 1]
+    assert rel_l2(got, ref) <= TOL
+    # every output sample, not only the norm: block seams are exact
+    assert np.max(np.abs(got - ref)) <= 20 * TOL * np.max(np.abs(ref))
+
+
+def test_convolve_real_overlap_save_float64_and_strided_batch():
+    import torch
+    rng = np.random.default_rng(9)
+    a = rng.uniform(-1, 1, 70000)
+    b = rng.uniform(-1, 1, 300)
+    got = np.empty(70299)
+    algofft.ConvolveReal(got, a, b)
+    assert rel_l2(got, np.convolve(a, b)) <= 1e-12
+    # strided batch: signals 70100 apart, outputs 70400 apart
+    count, na, ad, dd = 3, 70000, 70100, 70400
+    A = torch.from_numpy(rng.uniform(-1, 1, count * ad).astype(np.float32)).cuda()
+    K = torch.from_numpy(rng.uniform(-1, 1, 300).astype(np.float32)).cuda()
+    D = torch.zeros(count * dd, device="cuda")
+    algofft.ConvolveRealBatch(D, A, na, count, K, a_dist=ad, dst_dist=dd)
+    torch.cuda.synchronize()
+    Ah, Kh, Dh = A.cpu().numpy().astype(np.float64), K.cpu().numpy().astype(np.float64), D.cpu().numpy()
+    for i in range(count):
+        ref = np.convolve(Ah[i * ad:i * ad + na], Kh)
+        assert rel_l2(Dh[i * dd:i * dd + na + 299], ref) <= TOL
+        assert np.all(Dh[i * dd + na + 299:(i + 1) * dd] == 0)  # untouched gap
+
+
 def test_convolve_errors():
     a = np.ones(3, np.complex64)
     with pytest.raises(algofft.ErrLengthMismatch):
