@@ -72,6 +72,11 @@ gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int6
 bool column_sched(int64_t n, int prec, GenSched* s);
 gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const void* src, int64_t count,
                          int64_t dist, int64_t ncols, int64_t pitch, const void* tw_n, cudaStream_t st);
+// Power-of-two column batches (n <= 4096) through the compile-time column
+// tiles; cudaErrorNotSupported for other lengths.
+bool pow2_cols_supported(int64_t n);
+cudaError_t exec_pow2_cols(int prec, int dir, void* dst, const void* src, int64_t count, int64_t dist, int64_t ncols,
+                           int64_t pitch, const void* tw_n, int64_t n, cudaStream_t st);
 gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
                               int64_t odist, cudaStream_t st);
 

@@ -258,6 +258,11 @@ bool column_sched(int64_t n, int prec, GenSched* s) {
 
 gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const void* src, int64_t count,
                          int64_t dist, int64_t ncols, int64_t pitch, const void* tw_n, cudaStream_t st) {
+  if (pow2_cols_supported(s.n)) {
+    const cudaError_t e = exec_pow2_cols(prec, dir, dst, src, count, dist, ncols, pitch, tw_n, s.n, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_pow2_cols");
+    return GFFT_OK;
+  }
   BigTwiddle bt{nullptr, nullptr, 0};
   const double scale = 1.0 / double(s.n);
   cudaError_t e = prec == kC64

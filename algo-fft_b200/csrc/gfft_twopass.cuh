@@ -60,10 +60,14 @@ __device__ __forceinline__ C gload(const C* p) {
 // One Stockham stage of a column tile (see pow2_stage for the algebra).
 // Element (row, c) of the tile lives at sh[phys(row, c)]; global row r of
 // column c is at in[r*ISTRIDE + c].
+// ISTRIDE / OSTRIDE = 0 take the row pitch from `pitch` at run time.
 template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE>
 __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
                                           int t, int c, bool active, const C* __restrict__ tw,
-                                          typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2) {
+                                          typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2,
+                                          int64_t pitch = 0) {
+  const int64_t IS = ISTRIDE > 0 ? ISTRIDE : pitch;
+  const int64_t OS = OSTRIDE > 0 ? OSTRIDE : pitch;
   using S = ColShape<L, EPT, NC, sizeof(C)>;
   using SC = Sched<L, EPT>;
   constexpr int T = S::T;
@@ -79,7 +83,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int r = 0; r < RS; ++r)
-          v[q * RS + r] = gload<LOADK>(in + int64_t(t + q * T + r * STRIDE) * ISTRIDE + c);
+          v[q * RS + r] = gload<LOADK>(in + int64_t(t + q * T + r * STRIDE) * IS + c);
     } else {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
@@ -104,7 +108,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
         for (int r = 0; r < RS; ++r) {
           C o = v[q * RS + r];
           if constexpr (DIR > 0) o = cscale(o, scale);
-          st_stream(out + int64_t(t + q * T + r * P) * OSTRIDE + c, o);
+          st_stream(out + int64_t(t + q * T + r * P) * OS + c, o);
         }
     }
   } else if constexpr (LAST) {
@@ -146,7 +150,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
     }
     __syncthreads();
     col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE>(v, in, out, sh, t, c, active, tw, scale,
-                                                                         bt, n2);
+                                                                         bt, n2, pitch);
   }
 }
 
