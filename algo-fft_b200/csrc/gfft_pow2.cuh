@@ -123,6 +123,33 @@ __device__ __forceinline__ void pow2_fft(C* sh, int t, const C* __restrict__ tw,
   pow2_stage<C, N, EPT, DIR, 1>(v, sh, t, tw, ld, st);
 }
 
+// L2 prefetch of the inputs of CTA blockIdx + ahead (B transforms of `len`
+// elements, `idist` apart), issued by the CTA's threads before its own work;
+// ahead = co-resident CTAs, so the data lands about one CTA lifetime early.
+template <int B, int TPB, typename C>
+__device__ __forceinline__ void prefetch_ahead(const C* src, int64_t count, int64_t idist, int64_t len,
+                                               int64_t ahead) {
+  if (ahead <= 0) return;
+  const int64_t b2 = (int64_t(blockIdx.x) + ahead) * B;
+  if (b2 >= count) return;
+  const int nb = int(count - b2 < B ? count - b2 : B);
+  if (idist == len)
+    prefetch_range(src + b2 * idist, int64_t(nb) * len * int64_t(sizeof(C)), threadIdx.x, TPB);
+  else
+    for (int j = 0; j < nb; ++j) prefetch_range(src + (b2 + j) * idist, len * int64_t(sizeof(C)), threadIdx.x, TPB);
+}
+
+// Co-resident CTAs of a kernel on the current device (the prefetch distance).
+template <typename F>
+inline int64_t resident_ctas(F* fn, int tpb, int smem) {
+  int dev = 0, sms = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, smem);
+  cudaGetLastError();
+  return int64_t(sms) * (occ > 0 ? occ : 1);
+}
+
 template <typename C>
 struct GlobalLoad {
   static constexpr bool kShared = false;
@@ -157,17 +184,7 @@ __global__ void __launch_bounds__(Pow2Shape<N, EPT, sizeof(C)>::TPB)
 k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const C* __restrict__ tw,
        typename RealOf<C>::type scale, int64_t ahead) {
   using S = Pow2Shape<N, EPT, sizeof(C)>;
-  if (ahead > 0) {
-    const int64_t b2 = (int64_t(blockIdx.x) + ahead) * S::B;
-    if (b2 < count) {
-      const int nb = int(count - b2 < S::B ? count - b2 : S::B);
-      if (idist == N)
-        prefetch_range(src + b2 * idist, int64_t(nb) * N * int64_t(sizeof(C)), threadIdx.x, S::TPB);
-      else
-        for (int j = 0; j < nb; ++j)
-          prefetch_range(src + (b2 + j) * idist, int64_t(N) * int64_t(sizeof(C)), threadIdx.x, S::TPB);
-    }
-  }
+  prefetch_ahead<S::B, S::TPB>(src, count, idist, N, ahead);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sh = reinterpret_cast<C*>(smem_raw) + (threadIdx.x / S::T) * S::STRIDE;
   const int t = threadIdx.x % S::T;

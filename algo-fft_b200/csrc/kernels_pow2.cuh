@@ -13,14 +13,7 @@ cudaError_t launch_pow2(const void* src, void* dst, int64_t count, int64_t idist
   if (blocks <= 0) return cudaSuccess;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   // co-resident CTAs on this device: the prefetch distance
-  static const int64_t resident = [] {
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, &k_pow2<C, N, EPT, DIR>, S::TPB, S::SMEM);
-    cudaGetLastError();
-    return int64_t(sms) * (occ > 0 ? occ : 1);
-  }();
+  static const int64_t resident = resident_ctas(&k_pow2<C, N, EPT, DIR>, S::TPB, S::SMEM);
   const int64_t ahead = blocks > resident ? resident : 0;
   k_pow2<C, N, EPT, DIR><<<unsigned(blocks), S::TPB, S::SMEM, st>>>(
       static_cast<const C*>(src), static_cast<C*>(dst), count, idist, odist,
