@@ -228,7 +228,7 @@ def test_large_in_place_and_many_groups(n):
     assert rel_l2(got, ref) <= tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 20])
+@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 20, 2 ** 22, 2 ** 24])
 def test_every_variant_matches_oracle(n):
     count = max(2, (1 << 20) // n)
     x = seeded_complex(n * count, seed=3 + n % 101)
@@ -268,3 +268,4 @@ def test_forced_strategy_classes():
         assert "-tp-" in p.Algorithm()
     with algofft.NewPlanWithOptions(n, algofft.PlanOptions(Strategy=algofft.KernelStockham)) as p:
         assert "-p2-" in p.Algorithm()
+
