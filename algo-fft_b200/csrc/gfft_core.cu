@@ -6,6 +6,7 @@
 #include <vector>
 #include "gfft_internal.h"
 #include "gfft_math.cuh"
+#include "gfft_threepass.cuh"
 #include "gfft_twopass.cuh"
 
 namespace gfft {
@@ -22,7 +23,19 @@ static std::vector<TwoPassKernel>& twopass_table() {
   return t;
 }
 
+static std::vector<ThreePassKernel>& threepass_table() {
+  static std::vector<ThreePassKernel> t;
+  return t;
+}
+
 void register_pow2(const Pow2Kernel& k) { pow2_table().push_back(k); }
+void register_threepass(const ThreePassKernel& k) { threepass_table().push_back(k); }
+
+const ThreePassKernel* find_threepass(int prec, int64_t n, int dir) {
+  for (const auto& k : threepass_table())
+    if (k.prec == prec && int64_t(k.n1) * k.m1 * k.m2 == n && k.dir == dir) return &k;
+  return nullptr;
+}
 void register_twopass(const TwoPassKernel& k) { twopass_table().push_back(k); }
 
 const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te, int emax) {
@@ -76,6 +89,12 @@ cudaError_t prepare_kernels() {
       }
     }
   }
+  for (const auto& k : threepass_table())
+    if (k.smem > 48 * 1024)
+      for (const void* f : k.func) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+        if (e != cudaSuccess) return e;
+      }
   done.push_back(dev);
   return cudaSuccess;
 }
@@ -227,6 +246,41 @@ static gfft_status init_twopass(PlanCore* c, const TwoPassKernel* f, const TwoPa
   return GFFT_OK;
 }
 
+// Three-pass plan: W_N1 | W_M1 | W_M2 | split W_N | split W_M in one
+// allocation.
+static gfft_status init_threepass(PlanCore* c, const ThreePassKernel* f, const ThreePassKernel* inv) {
+  const int64_t n = c->n, n1 = f->n1, m1 = f->m1, m2 = f->m2, m = m1 * m2;
+  const size_t es = elem_bytes(c->prec);
+  const int shn = (ilog2(n) + 1) / 2, shm = (ilog2(m) + 1) / 2;
+  const int64_t nlo = int64_t(1) << shn, nhi = n >> shn, mlo = int64_t(1) << shm, mhi = m >> shm;
+  const int64_t total = n1 + m1 + m2 + nlo + nhi + mlo + mhi;
+  GFFT_CUDA(cudaMalloc(&c->tw, size_t(total) * es));
+  char* base = static_cast<char*>(c->tw);
+  int64_t off = 0;
+  auto put = [&](int64_t len, int64_t cnt, int64_t step, const void** where) -> gfft_status {
+    gfft_status s = fill_twiddles(c->prec, base + off * es, len, cnt, step, 0);
+    if (where) *where = base + off * es;
+    off += cnt;
+    return s;
+  };
+  gfft_status s = put(n1, n1, 1, &c->tw1);
+  if (s == GFFT_OK) s = put(m1, m1, 1, &c->tw2);
+  if (s == GFFT_OK) s = put(m2, m2, 1, &c->tw3);
+  if (s == GFFT_OK) s = put(n, nlo, 1, &c->bt_lo);
+  if (s == GFFT_OK) s = put(n, nhi, nlo, &c->bt_hi);
+  if (s == GFFT_OK) s = put(m, mlo, 1, &c->btm_lo);
+  if (s == GFFT_OK) s = put(m, mhi, mlo, &c->btm_hi);
+  if (s != GFFT_OK) return s;
+  GFFT_CUDA(cudaStreamSynchronize(0));
+  c->bt_shift = shn;
+  c->btm_shift = shm;
+  c->t3[0] = f;
+  c->t3[1] = inv;
+  c->algo = Algo::ThreePass;
+  c->name = "gpu-sm100-tp3-" + std::to_string(n1) + "x" + std::to_string(m1) + "x" + std::to_string(m2);
+  return GFFT_OK;
+}
+
 static std::string pow2_token(int n, int ept) {
   return "gpu-sm100-p2-n" + std::to_string(n) + "-e" + std::to_string(ept);
 }
@@ -242,6 +296,8 @@ std::vector<std::string> variant_tokens(int prec, int64_t n) {
     if (n <= (prec == kC64 ? 16384 : 8192))
       for (const Pow2Kernel* k : pow2_variants(prec, int(n), -1)) v.push_back(pow2_token(k->n, k->ept));
     for (const TwoPassKernel* k : twopass_variants(prec, n, -1)) v.push_back(twopass_token(k));
+    if (const ThreePassKernel* k = find_threepass(prec, n, -1))
+      v.push_back("gpu-sm100-tp3-" + std::to_string(k->n1) + "x" + std::to_string(k->m1) + "x" + std::to_string(k->m2));
   } else if (n > 1 && is_smooth7(n)) {
     // runtime-radix schedules (single CTA when it fits, two passes when n
     // has a 7-smooth divisor >= 2 below sqrt n) against Bluestein
@@ -280,6 +336,11 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     const TwoPassKernel* f = find_twopass(prec, n, -1, te, e);
     const TwoPassKernel* i = find_twopass(prec, n, +1, te, e);
     if (f && i) return init_twopass(c, f, i);
+  }
+  if (std::sscanf(tok.c_str(), "gpu-sm100-tp3-%dx%dx%d", &a, &b, &te) == 3 && int64_t(a) * b * te == n) {
+    const ThreePassKernel* f = find_threepass(prec, n, -1);
+    const ThreePassKernel* i = find_threepass(prec, n, +1);
+    if (f && i && f->n1 == a && f->m1 == b && f->m2 == te) return init_threepass(c, f, i);
   }
   long long ln = 0, l1 = 0, l2 = 0;
   if (std::sscanf(tok.c_str(), "gpu-sm100-mixed-n%lld", &ln) == 1 && ln == n && is_smooth7(n)) return init_generic(c);
@@ -420,6 +481,41 @@ static gfft_status exec_twopass(const PlanCore* c, int dir, void* dst, const voi
   return GFFT_OK;
 }
 
+// Three-pass execution: per chunk of up to 1 GiB of intermediate, one
+// launch per pass (pass 2 works in place on the intermediate).
+static gfft_status exec_threepass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                                  int64_t idist, int64_t odist, cudaStream_t st) {
+  const ThreePassKernel* k = c->t3[dir < 0 ? 0 : 1];
+  const int64_t tbytes = c->n * int64_t(elem_bytes(c->prec));
+  const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(1) << 30) / tbytes));
+  void* ws = nullptr;
+  GFFT_CUDA(ws_alloc(&ws, size_t(nb) * size_t(tbytes), st));
+  ThreePassParams p{};
+  p.src = src;
+  p.dst = dst;
+  p.scratch = ws;
+  p.idist = idist;
+  p.odist = odist;
+  p.tw1 = c->tw1;
+  p.tw2 = c->tw2;
+  p.tw3 = c->tw3;
+  p.bt.lo = c->bt_lo;
+  p.bt.hi = c->bt_hi;
+  p.bt.shift = c->bt_shift;
+  p.btm.lo = c->btm_lo;
+  p.btm.hi = c->btm_hi;
+  p.btm.shift = c->btm_shift;
+  p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+  cudaError_t e = cudaSuccess;
+  for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += nb) {
+    const int64_t m = std::min(nb, count - b0);
+    for (int pass = 1; pass <= 3 && e == cudaSuccess; ++pass) e = k->launch(p, pass, b0, m, st);
+  }
+  cudaFreeAsync(ws, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_tp3");
+  return GFFT_OK;
+}
+
 gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
                       int64_t odist, cudaStream_t st) {
   if (count <= 0) return GFFT_OK;
@@ -438,6 +534,8 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
     }
     case Algo::TwoPass:
       return exec_twopass(c, dir, dst, src, count, idist, odist, st);
+    case Algo::ThreePass:
+      return exec_threepass(c, dir, dst, src, count, idist, odist, st);
     case Algo::Generic:
     case Algo::GenTwoPass:
     case Algo::Bluestein:

@@ -21,7 +21,7 @@ gfft_status cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::gfft::cuda_status(e_, #call); \
   } while (0)
 
-enum class Algo { Trivial, Pow2Smem, TwoPass, Generic, GenTwoPass, Bluestein, TensorCore };
+enum class Algo { Trivial, Pow2Smem, TwoPass, ThreePass, Generic, GenTwoPass, Bluestein, TensorCore };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
 // FP64 and rounded to the element type (internal/math/twiddle.go:8-21).
@@ -37,6 +37,12 @@ struct PlanCore {
   std::string name;
   // two-pass schedule
   const TwoPassKernel* tp[2] = {nullptr, nullptr};
+  // three-pass schedule: kernels, W_M2 table (tw1 = W_N1, tw2 = W_M1), split W_M
+  const ThreePassKernel* t3[2] = {nullptr, nullptr};
+  const void* tw3 = nullptr;
+  const void* btm_lo = nullptr;
+  const void* btm_hi = nullptr;
+  int btm_shift = 0;
   const void* tw1 = nullptr;                     // W_N1
   const void* tw2 = nullptr;                     // W_N2
   const void* bt_lo = nullptr;

@@ -34,7 +34,18 @@ struct TwoPassKernel {
   cudaError_t (*split)(const TwoPassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st);
 };
 
+// Three-pass kernels (k_tp3) of one (precision, N1 x M1 x M2, dir).
+struct ThreePassParams;
+struct ThreePassKernel {
+  int prec, n1, m1, m2, dir;
+  int tpb, smem;
+  const void* func[3];  // passes 1..3
+  cudaError_t (*launch)(const ThreePassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st);
+};
+
 void register_pow2(const Pow2Kernel& k);
+void register_threepass(const ThreePassKernel& k);
+const ThreePassKernel* find_threepass(int prec, int64_t n, int dir);
 void register_twopass(const TwoPassKernel& k);
 const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te = 0, int emax = 0);
 std::vector<const TwoPassKernel*> twopass_variants(int prec, int64_t n, int dir);

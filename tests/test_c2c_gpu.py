@@ -269,3 +269,16 @@ def test_forced_strategy_classes():
     with algofft.NewPlanWithOptions(n, algofft.PlanOptions(Strategy=algofft.KernelStockham)) as p:
         assert "-p2-" in p.Algorithm()
 
+
+
+@pytest.mark.parametrize("n", [2 ** 21, 2 ** 24])
+def test_three_pass_complex128(n):
+    # the three-pass schedule (N = N1 x M1 x M2, factors <= 256) in complex128
+    tok = [t for t in algofft.Variants(n, algofft.COMPLEX128) if "-tp3-" in t]
+    assert tok
+    x = seeded_complex(2 * n, seed=n % 89, dtype=np.complex128)
+    with algofft.Plan(n, algofft.COMPLEX128, variant=tok[0]) as p:
+        y = _run(p, x, 2)
+        back = _run(p, y, 2, inverse=True)
+    assert rel_l2(y[:n], np.fft.fft(x[:n])) <= tol_c2c(n, True)
+    assert rel_l2(back, x) <= 2 * tol_c2c(n, True)
