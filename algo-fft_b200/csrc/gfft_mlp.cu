@@ -5,7 +5,8 @@
 // shape: log2 n, the exponents of 2/3/5/7 in n, log2 of n's largest prime
 // factor, log2 batch, precision, log2 stride, real/complex; the candidate:
 // one-hot kind p2/tp/mixed/bluestein plus two numeric shape parameters of
-// the variant), standardized with stored means and deviations, through
+// the variant; the three-pass form is kind tp with both parameters 0),
+// standardized with stored means and deviations, through
 // 16 -> 64 -> 64 -> 1 with ReLU, to a standardized log(ns per element).
 // Plan creation with GFFT_PLANNER_LEARNED evaluates every candidate of the
 // length in one inference launch and takes the smallest prediction; the
@@ -273,6 +274,8 @@ static bool plan_features(int prec, int64_t n, int64_t batch, int64_t stride, in
     f[11] = 1.f;
     f[14] = float(ilog2f(e));
     f[15] = float(ilog2f(te));
+  } else if (std::sscanf(tok.c_str(), "gpu-sm100-tp3-%dx%dx%d", &a, &b, &te) == 3) {
+    f[11] = 1.f;  // a multi-pass schedule with no tile parameters: the three-pass form
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixed2-%lldx%lld", &l1, &l2) == 2) {
     f[12] = 1.f;
     f[14] = 1.f;

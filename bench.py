@@ -41,17 +41,20 @@ BUF_BYTES = 1 << 30                      # one 1 GiB batch per length
 SWEEP = [2 ** k for k in range(4, 25)]
 WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^4..2^24, 1 GiB batch per N"
 
-# DRAM bytes per transform (read + write) of the two-pass kernels, from
-# ncu captures of small batches (profiles/k_tp_split_twopass.md); used to
-# scale `roofline.traffic` to a full launch.
-TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6}
+# DRAM bytes per transform (read + write, all passes) of the multi-pass
+# plans, from ncu captures of small batches (profiles/k_tp_split_n16777216.md,
+# profiles/k_tp3_n8388608.md); used to scale `roofline.traffic` to a launch.
+TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6,
+                         "gpu-sm100-tp3-256x256x128": 359.4e6}
 
 
 def launches_of(algorithm: str, count: int, n: int, es: int) -> int:
-    """Kernel launches of one ForwardBatch of this plan."""
-    if "-tp-" in algorithm:
+    """Kernel launches of one ForwardBatch of this plan (multi-pass plans:
+    one launch per pass per chunk of up to 1 GiB of intermediate)."""
+    passes = 3 if "-tp3-" in algorithm else 2 if "-tp-" in algorithm else 1
+    if passes > 1:
         chunk = max(1, min(count, (1 << 30) // (n * es)))
-        return 2 * ((count + chunk - 1) // chunk)
+        return passes * ((count + chunk - 1) // chunk)
     return 1
 
 
@@ -439,7 +442,9 @@ def main():
     dom_bytes = bytes_per_transform(dom) * bufs[dom][2] / dom_launches  # algorithmic bytes per launch
     peak, peak_kind = peak_hbm()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    if "-tp-" in dom_alg:
+    if "-tp3-" in dom_alg:
+        kname = f"k_tp3 (three passes, one launch each; N={dom}, {dom_alg})"
+    elif "-tp-" in dom_alg:
         kname = f"k_tp_split (two-pass, pass 1 and pass 2 alternate; N={dom}, {dom_alg})"
     else:
         kname = f"k_pow2 (single pass; N={dom}, {dom_alg})"
