@@ -228,7 +228,7 @@ def test_large_in_place_and_many_groups(n):
     assert rel_l2(got, ref) <= tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 20, 2 ** 22, 2 ** 24])
+@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 16, 2 ** 17, 2 ** 20, 2 ** 22, 2 ** 24])
 def test_every_variant_matches_oracle(n):
     count = max(2, (1 << 20) // n)
     x = seeded_complex(n * count, seed=3 + n % 101)
@@ -282,3 +282,4 @@ def test_three_pass_complex128(n):
         back = _run(p, y, 2, inverse=True)
     assert rel_l2(y[:n], np.fft.fft(x[:n])) <= tol_c2c(n, True)
     assert rel_l2(back, x) <= 2 * tol_c2c(n, True)
+
