@@ -27,39 +27,41 @@ gfft_status cuda_status(cudaError_t e, const char* what) {
 
 static cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
-// Host-slice path: the batch moves in chunks of about 64 MB through two
-// streams and two staging buffers (workspace pool): chunk k's copy in, its
-// transforms and its copy out are ordered on stream k % 2, so the copy out
-// of one chunk overlaps the copy in of the next (both directions of the
-// host link at once) and the transforms hide under the copies.  With
-// pageable host memory the copies still complete correctly but cannot
-// overlap.  Returns after the last copy out.
+// Host-slice path: the batch moves in chunks of about 64 MB through three
+// streams and three staging buffers (workspace pool): chunk k's copy in, its
+// transforms and its copy out are ordered on stream k % 3, so the copy out
+// of one chunk, the transforms of the next and the copy in of the one
+// after run at once (both directions of the host link busy, transforms
+// hidden under the copies).  With pageable host memory the copies still
+// complete correctly but cannot overlap.  Returns after the last copy out.
 static gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count) {
+  constexpr int kLanes = 3;
   const size_t tb = size_t(p->core.n) * elem_bytes(p->core.prec);
   const int64_t per = std::max<int64_t>(1, std::min<int64_t>(count, int64_t((size_t(64) << 20) / tb)));
-  cudaStream_t st[2] = {nullptr, nullptr};
-  void* d[2] = {nullptr, nullptr};
+  cudaStream_t st[kLanes] = {};
+  void* d[kLanes] = {};
   gfft_status s = GFFT_OK;
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
-  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = ws_alloc(&d[i], size_t(per) * tb, st[i]);
+  for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
+  for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = ws_alloc(&d[i], size_t(per) * tb, st[i]);
   if (e != cudaSuccess) s = cuda_status(e, "host path setup");
   int k = 0;
   for (int64_t b0 = 0; b0 < count && s == GFFT_OK; b0 += per, ++k) {
     const int64_t m = std::min(per, count - b0);
     const size_t bytes = size_t(m) * tb, off = size_t(b0) * tb;
-    cudaStream_t q = st[k & 1];
-    e = cudaMemcpyAsync(d[k & 1], static_cast<const char*>(src) + off, bytes, cudaMemcpyHostToDevice, q);
+    cudaStream_t q = st[k % kLanes];
+    void* buf = d[k % kLanes];
+    e = cudaMemcpyAsync(buf, static_cast<const char*>(src) + off, bytes, cudaMemcpyHostToDevice, q);
     if (e != cudaSuccess) {
       s = cuda_status(e, "cudaMemcpyAsync(H2D)");
       break;
     }
-    s = core_exec(&p->core, dir, d[k & 1], d[k & 1], m, p->core.n, p->core.n, q);
+    s = core_exec(&p->core, dir, buf, buf, m, p->core.n, p->core.n, q);
     if (s != GFFT_OK) break;
-    e = cudaMemcpyAsync(static_cast<char*>(dst) + off, d[k & 1], bytes, cudaMemcpyDeviceToHost, q);
+    e = cudaMemcpyAsync(static_cast<char*>(dst) + off, buf, bytes, cudaMemcpyDeviceToHost, q);
     if (e != cudaSuccess) s = cuda_status(e, "cudaMemcpyAsync(D2H)");
   }
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kLanes; ++i) {
     if (!st[i]) continue;
     if (d[i]) cudaFreeAsync(d[i], st[i]);
     e = cudaStreamSynchronize(st[i]);

@@ -83,6 +83,12 @@ gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const 
 bool pow2_cols_supported(int64_t n);
 cudaError_t exec_pow2_cols(int prec, int dir, void* dst, const void* src, int64_t count, int64_t dist, int64_t ncols,
                            int64_t pitch, const void* tw_n, int64_t n, cudaStream_t st);
+// Bluestein as one fused kernel when the FFT length M fits one CTA (M a
+// power of two <= 16384 complex64, <= 8192 complex128).
+bool bluestein_fused_supported(int prec, int64_t M);
+cudaError_t exec_bluestein_fused(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
+                                 int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw,
+                                 double scale, cudaStream_t st);
 gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
                               int64_t odist, cudaStream_t st);
 

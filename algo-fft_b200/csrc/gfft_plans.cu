@@ -352,6 +352,15 @@ static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const v
   const size_t es = elem_bytes(c->prec);
   const int64_t n = c->n, M = c->bm;
   const int d = dir < 0 ? 0 : 1;
+  // one fused launch when FFT_M fits one CTA (the sub-plan is single-pass,
+  // so its W_M table serves the fused stages)
+  if (c->sub->algo == Algo::Pow2Smem && bluestein_fused_supported(c->prec, M)) {
+    const double fscale = (dir < 0 ? 1.0 : 1.0 / double(n)) / double(M);
+    const cudaError_t fe = exec_bluestein_fused(c->prec, M, src, dst, count, idist, odist, n, c->bs_w[d], c->bs_f[d],
+                                                c->sub->tw, fscale, st);
+    if (fe != cudaSuccess) return cuda_status(fe, "k_bs_fused");
+    return GFFT_OK;
+  }
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
   void* work = nullptr;
   GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&work), size_t(chunk) * size_t(M) * es, st));
