@@ -85,9 +85,25 @@ struct RepackLoad {
   }
 };
 
+// The packed input of the inverse from bins staged in shared memory
+// (X[0..h) at the padded positions, X[h] in a register).
+template <typename C, int H, int EPT>
+struct RepackSharedLoad {
+  static constexpr bool kShared = true;
+  const C* sh;
+  const C* wt;
+  C x0, xh;
+  __device__ __forceinline__ C operator()(int e) const {
+    using S = Pow2Shape<H, EPT, sizeof(C)>;
+    return c2r_packed(sh[S::pad(e)], sh[S::pad(e == 0 ? 0 : H - e)], x0, xh, __ldg(wt + e), e);
+  }
+};
+
 // C2R: src holds h+1 bins of transform b at src + b*idist; dst gets the N
 // reals at dst + b*odist (complex units).  scale = 1/h (the half-length
-// inverse of the reference, plan_real_generic.go:333).
+// inverse of the reference, plan_real_generic.go:333).  The bins are read
+// once, coalesced, into shared memory; the packing of the first stage pairs
+// bins k and h-k from there.
 template <typename C, int H, int EPT>
 __global__ void __launch_bounds__(Pow2Shape<H, EPT, sizeof(C)>::TPB)
 k_c2r_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const C* __restrict__ tw,
@@ -99,7 +115,14 @@ k_c2r_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, co
   const int64_t b = int64_t(blockIdx.x) * S::B + threadIdx.x / S::T;
   const bool valid = b < count;
   const C* X = src + (valid ? b * idist : 0);
-  RepackLoad<C> ld{X, wt, H, valid, valid ? X[0] : C{0, 0}, valid ? X[H] : C{0, 0}};
+#pragma unroll
+  for (int i = 0; i < EPT; ++i) {
+    const int k = t + i * S::T;
+    sh[S::pad(k)] = valid ? ld_stream(X + k) : C{0, 0};
+  }
+  const C xh = valid ? X[H] : C{0, 0};
+  xsync<S::T>();
+  RepackSharedLoad<C, H, EPT> ld{sh, wt, sh[0], xh};
   GlobalStore<C, true> st{dst + (valid ? b * odist : 0), valid, scale};
   pow2_fft<C, H, EPT, +1>(sh, t, tw, ld, st);
 }
