@@ -7,7 +7,7 @@ there is no CPU fallback: if the library is missing the import fails.
 from ._lib import (ErrCuda, ErrInvalidArgument, ErrInvalidLength, ErrInvalidSpectrum, ErrInvalidStride,
                    ErrLengthMismatch, ErrNilSlice, ErrNoDevice, ErrNotImplemented, ErrOutOfMemory, ErrTimeout,
                    ErrWisdom, GfftError, LIB_PATH, check, lib)
-from .plan import (COMPLEX64, COMPLEX128, KernelAuto, KernelBluestein, KernelDIT, KernelEightStep, KernelRecursive,
+from .plan import (COMPLEX64, COMPLEX128, Executor, KernelAuto, KernelBluestein, KernelDIT, KernelEightStep, KernelRecursive,
                    KernelSixStep, KernelStockham, NewPlan, NewPlan32, NewPlan64, NewPlanT, NewPlanWithOptions, Plan,
                    PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerLearned, PlannerMeasure,
                    PlannerPatient)
@@ -15,6 +15,8 @@ from .plan import (COMPLEX64, COMPLEX128, KernelAuto, KernelBluestein, KernelDIT
 from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, ConvolveReal, ConvolveRealBatch,
                        Correlate, Correlate128, CrossCorrelate, CrossCorrelate128)
 from .nd import NewPlan2D, NewPlan3D, NewPlanND, NewPlanReal2D, NewPlanReal3D, PlanND
+from .plan_helpers import (ClearPlanPool, FastPlan, NewFastPlan, NewPlanner, NewPlanPooled,
+                           NewPlanPooledWithOptions, Plan1D, Planner)
 from .real import NewPlanReal, NewPlanReal32, NewPlanReal64, NewPlanRealWithOptions, PlanReal
 from .uneven import PlanUneven, uneven_lengths
 from .wisdom import (Autotune, ClearWisdom, ExportWisdom, ExportWisdomToString, ImportWisdom,

@@ -151,6 +151,9 @@ SIGNATURES = {
     "gfft_planner_load_model": (I32, [CHARP]),
     "gfft_planner_has_model": (I32, []),
     "gfft_planner_choose": (I32, [I32, I64, I64, I64, I32, ctypes.c_char_p, ctypes.c_size_t]),
+    "gfft_plan_clone": (I32, [PP, P]),
+    "gfft_plan_new_pooled": (I32, [PP, I32, I64, ctypes.POINTER(PlanOptionsC)]),
+    "gfft_plan_pool_clear": (None, []),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

@@ -80,9 +80,25 @@ class Plan:
             c_opts = self._opts.to_c()
             check(lib().gfft_plan_new(ctypes.byref(self._h), precision, n, ctypes.byref(c_opts)))
 
+    @classmethod
+    def _wrap(cls, h, precision: int, opts: PlanOptions) -> "Plan":
+        p = cls.__new__(cls)
+        p._h, p.precision, p._opts = h, precision, opts
+        return p
+
     def Check(self) -> None:
         """Raises ErrTimeout if a bounded device wait of this plan expired."""
         check(lib().gfft_plan_check(self._h))
+
+    def Clone(self) -> "Plan":
+        """plan.go:1300 Clone: an independent plan with the same schedule."""
+        h = ctypes.c_void_p()
+        check(lib().gfft_plan_clone(ctypes.byref(h), self._h))
+        return Plan._wrap(h, self.precision, self._opts)
+
+    def NewExecutor(self) -> "Executor":
+        """executor.go:11 NewExecutor."""
+        return Executor(self)
 
     # -- lifecycle ---------------------------------------------------------
     def Close(self) -> None:
@@ -186,6 +202,51 @@ class Plan:
             return None
         check(getattr(lib(), fn)(self._h, dp, dl, sp, sl, stride, _stream(dst)))
         return None
+
+
+class Executor:
+    """Executor[T] (executor.go:11-40): one caller's handle on a plan.  The
+    GPU plan is reentrant (no shared scratch), so an executor's part is its
+    own CUDA stream: device calls run on it, ordered after the caller's
+    current stream and joined back into it, so executors of one plan run
+    concurrently.  Host buffers take the synchronous host path."""
+
+    def __init__(self, plan: Plan):
+        self.plan = plan
+        self._stream = None
+
+    def _run(self, fn, *args):
+        if not _is_device(args[0]):
+            return fn(*args)
+        import torch
+        if self._stream is None:
+            self._stream = torch.cuda.Stream(device=args[0].device)
+        cur = torch.cuda.current_stream(args[0].device)
+        self._stream.wait_stream(cur)
+        with torch.cuda.stream(self._stream):
+            fn(*args)
+        cur.wait_stream(self._stream)
+        return None
+
+    def Forward(self, dst, src):
+        """executor.go:16."""
+        return self._run(self.plan.Forward, dst, src)
+
+    def Inverse(self, dst, src):
+        """executor.go:21."""
+        return self._run(self.plan.Inverse, dst, src)
+
+    def ForwardInPlace(self, data):
+        """executor.go:26."""
+        return self._run(self.plan.InPlace, data)
+
+    def InverseInPlace(self, data):
+        """executor.go:31."""
+        return self._run(self.plan.InverseInPlace, data)
+
+    def Close(self) -> None:
+        """executor.go:36 (the plan stays open)."""
+        self._stream = None
 
 
 def NewPlanT(n: int, precision: int = COMPLEX64) -> Plan:

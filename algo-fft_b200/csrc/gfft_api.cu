@@ -9,6 +9,9 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include "gfft_internal.h"
 
 namespace gfft {
@@ -99,6 +102,7 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts = o;
+  p->precision = precision;
   PlanHint hint;
   hint.planner = o.planner;
   hint.batch = o.batch;
@@ -112,10 +116,94 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
   return GFFT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Pooled plans (NewPlanPooled, plan.go:1040-1118): closed plans wait here,
+// keyed by (device, precision, n, planner, strategy), for the next request
+// of the same shape, so a caller that creates and closes plans in a loop
+// does not rebuild twiddle tables each time.
+struct PoolKey {
+  int device, prec;
+  int64_t n;
+  int planner, strategy;
+  bool operator<(const PoolKey& o) const {
+    return std::tie(device, prec, n, planner, strategy) < std::tie(o.device, o.prec, o.n, o.planner, o.strategy);
+  }
+};
+std::mutex g_pool_mu;
+std::map<PoolKey, std::vector<gfft_plan*>> g_pool;
+}  // namespace
+
+extern "C" {
+
+gfft_status gfft_plan_new_pooled(gfft_plan** out, int32_t precision, int64_t n, const gfft_plan_options* opts) {
+  clear_error();
+  if (!out) return GFFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  gfft_plan_options o{};
+  if (opts) o = *opts;
+  if (o.batch > 1 || o.stride > 0) return gfft_plan_new(out, precision, n, opts);  // layouts are not pooled
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    auto it = g_pool.find(PoolKey{o.device, precision, n, o.planner, o.strategy});
+    if (it != g_pool.end() && !it->second.empty()) {
+      *out = it->second.back();
+      it->second.pop_back();
+      return GFFT_OK;
+    }
+  }
+  gfft_status s = gfft_plan_new(out, precision, n, opts);
+  if (s == GFFT_OK) (*out)->pooled = true;
+  return s;
+}
+
+void gfft_plan_pool_clear(void) {
+  std::vector<gfft_plan*> all;
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    for (auto& kv : g_pool)
+      for (gfft_plan* p : kv.second) all.push_back(p);
+    g_pool.clear();
+  }
+  for (gfft_plan* p : all) {
+    core_free(&p->core);
+    delete p;
+  }
+}
+
 void gfft_plan_close(gfft_plan* plan) {
   if (!plan) return;
+  if (plan->pooled) {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    g_pool[PoolKey{plan->opts.device, plan->precision, plan->core.n, plan->opts.planner, plan->opts.strategy}]
+        .push_back(plan);
+    return;
+  }
   core_free(&plan->core);
   delete plan;
+}
+
+gfft_status gfft_plan_clone(gfft_plan** out, const gfft_plan* src) {
+  clear_error();
+  if (!out || !src) return GFFT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  GFFT_CUDA(cudaSetDevice(src->core.device));
+  auto* p = new (std::nothrow) gfft_plan;
+  if (!p) return GFFT_ERR_OUT_OF_MEMORY;
+  p->opts = src->opts;
+  p->precision = src->precision;
+  // the same schedule, tables rebuilt for the copy
+  gfft_status s = src->core.n == 1 ? core_init(&p->core, src->precision, 1, src->core.device)
+                                   : core_init_variant(&p->core, src->precision, src->core.n, src->core.device,
+                                                       src->core.name);
+  if (s != GFFT_OK) {
+    core_free(&p->core);
+    delete p;
+    return s;
+  }
+  *out = p;
+  return GFFT_OK;
 }
 
 int64_t gfft_plan_len(const gfft_plan* plan) { return plan ? plan->core.n : 0; }
@@ -266,6 +354,7 @@ gfft_status gfft_plan_new_variant(gfft_plan** out, int32_t precision, int64_t n,
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts.device = dev;
+  p->precision = precision;
   gfft_status s = core_init_variant(&p->core, precision, n, dev, token);
   if (s != GFFT_OK) {
     core_free(&p->core);

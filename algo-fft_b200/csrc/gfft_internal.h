@@ -146,6 +146,8 @@ inline size_t elem_bytes(int prec) { return prec == kC64 ? 8 : 16; }
 struct gfft_plan {
   gfft::PlanCore core;
   gfft_plan_options opts{};
+  int32_t precision = 0;
+  bool pooled = false;  // Close returns it to the plan pool
 };
 
 namespace gfft {

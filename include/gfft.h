@@ -98,6 +98,20 @@ GFFT_API gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n
 
 /* Plan.Close (plan.go:1223).  NULL is ignored. */
 GFFT_API void gfft_plan_close(gfft_plan* plan);
+/* Clone (plan.go:1300): an independent plan with the same schedule (its
+ * tables rebuilt on the device; GPU plans keep no per-call scratch, so the
+ * copy exists for callers that want separately closable handles).  Closing
+ * either leaves the other intact. */
+GFFT_API gfft_status gfft_plan_clone(gfft_plan** out, const gfft_plan* src);
+/* NewPlanPooled / NewPlanPooledWithOptions (plan.go:1040-1118): like
+ * gfft_plan_new, but gfft_plan_close returns the plan to a process-wide pool
+ * keyed by (device, precision, n, planner, strategy) and the next pooled
+ * request of that shape reuses it instead of rebuilding its tables.  Batch
+ * layouts (opts->batch > 1 or opts->stride > 0) are not pooled.
+ * gfft_plan_pool_clear frees every pooled plan. */
+GFFT_API gfft_status gfft_plan_new_pooled(gfft_plan** out, int32_t precision, int64_t n,
+                                          const gfft_plan_options* opts);
+GFFT_API void gfft_plan_pool_clear(void);
 
 /* Plan.Len (plan.go:148). */
 GFFT_API int64_t gfft_plan_len(const gfft_plan* plan);
