@@ -7,9 +7,9 @@ there is no CPU fallback: if the library is missing the import fails.
 from ._lib import (ErrCuda, ErrInvalidArgument, ErrInvalidLength, ErrInvalidSpectrum, ErrInvalidStride,
                    ErrLengthMismatch, ErrNilSlice, ErrNoDevice, ErrNotImplemented, ErrOutOfMemory, ErrTimeout,
                    ErrWisdom, GfftError, LIB_PATH, check, lib)
-from .plan import (COMPLEX64, COMPLEX128, Executor, KernelAuto, KernelBluestein, KernelDIT, KernelEightStep, KernelRecursive,
+from .plan import (COMPLEX64, COMPLEX128, Executor, GetKernelStrategy, KernelAuto, KernelBluestein, KernelDIT, KernelEightStep, KernelRecursive,
                    KernelSixStep, KernelStockham, NewPlan, NewPlan32, NewPlan64, NewPlanT, NewPlanWithOptions, Plan,
-                   PlanOptions, PlannerEstimate, PlannerExhaustive, PlannerLearned, PlannerMeasure,
+                   PlanOptions, PlannerEstimate, RecordBenchmarkDecision, SetKernelStrategy, PlannerExhaustive, PlannerLearned, PlannerMeasure,
                    PlannerPatient)
 
 from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, ConvolveReal, ConvolveRealBatch,

@@ -154,6 +154,9 @@ SIGNATURES = {
     "gfft_plan_clone": (I32, [PP, P]),
     "gfft_plan_new_pooled": (I32, [PP, I32, I64, ctypes.POINTER(PlanOptionsC)]),
     "gfft_plan_pool_clear": (None, []),
+    "gfft_set_kernel_strategy": (None, [I32]),
+    "gfft_get_kernel_strategy": (I32, []),
+    "gfft_record_benchmark_decision": (None, [I64, I32]),
     "gfft_status_string": (CHARP, [I32]),
     "gfft_last_error": (CHARP, []),
     "gfft_device_count": (I32, [ctypes.POINTER(I32)]),

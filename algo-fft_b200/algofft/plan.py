@@ -249,6 +249,21 @@ class Executor:
         self._stream = None
 
 
+def SetKernelStrategy(strategy: int) -> None:
+    """plan.go:112 SetKernelStrategy (process-wide)."""
+    lib().gfft_set_kernel_strategy(strategy)
+
+
+def GetKernelStrategy() -> int:
+    """plan.go:117 GetKernelStrategy."""
+    return int(lib().gfft_get_kernel_strategy())
+
+
+def RecordBenchmarkDecision(n: int, strategy: int) -> None:
+    """plan.go:122 RecordBenchmarkDecision."""
+    lib().gfft_record_benchmark_decision(n, strategy)
+
+
 def NewPlanT(n: int, precision: int = COMPLEX64) -> Plan:
     """plan.go:596 NewPlanT[T]."""
     return Plan(n, precision)

@@ -106,6 +106,7 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
   PlanHint hint;
   hint.planner = o.planner;
   hint.batch = o.batch;
+  hint.user = true;
   gfft_status s = core_init(&p->core, precision, n, o.device, o.strategy, &hint);
   if (s != GFFT_OK) {
     core_free(&p->core);
@@ -182,6 +183,18 @@ void gfft_plan_close(gfft_plan* plan) {
   }
   core_free(&plan->core);
   delete plan;
+}
+
+void gfft_set_kernel_strategy(int32_t strategy) { set_kernel_strategy(strategy); }
+int32_t gfft_get_kernel_strategy(void) { return get_kernel_strategy(); }
+void gfft_record_benchmark_decision(int64_t n, int32_t strategy) {
+  // internal/planner/selection.go:42-60: lengths >= 1 and the four
+  // schedule strategies only
+  if (n <= 0) return;
+  if (strategy != GFFT_KERNEL_DIT && strategy != GFFT_KERNEL_STOCKHAM && strategy != GFFT_KERNEL_SIXSTEP &&
+      strategy != GFFT_KERNEL_EIGHTSTEP)
+    return;
+  record_decision(n, strategy);
 }
 
 gfft_status gfft_plan_clone(gfft_plan** out, const gfft_plan* src) {

@@ -1,5 +1,7 @@
 // Kernel registry, device twiddle generation and the 1-D schedule choice.
 #include <algorithm>
+#include <atomic>
+#include <map>
 #include <cstdlib>
 #include <cstdio>
 #include <mutex>
@@ -355,7 +357,34 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
   return GFFT_ERR_INVALID_ARGUMENT;
 }
 
+// SetKernelStrategy / RecordBenchmarkDecision (plan.go:110-125,
+// internal/planner/selection.go:22-60): a process-wide strategy that
+// overrides automatic selection for plans created with KernelAuto, and
+// per-length strategy classes used while selection is automatic.
+namespace {
+std::atomic<int> g_strategy{GFFT_KERNEL_AUTO};
+std::mutex g_decision_mu;
+std::map<int64_t, int> g_decisions;
+}  // namespace
+
+void set_kernel_strategy(int s) { g_strategy.store(s); }
+int get_kernel_strategy() { return g_strategy.load(); }
+void record_decision(int64_t n, int s) {
+  std::lock_guard<std::mutex> g(g_decision_mu);
+  g_decisions[n] = s;
+}
+
+static int recorded_decision(int64_t n) {
+  std::lock_guard<std::mutex> g(g_decision_mu);
+  auto it = g_decisions.find(n);
+  return it == g_decisions.end() ? GFFT_KERNEL_AUTO : it->second;
+}
+
 gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy, const PlanHint* hint) {
+  // the process-wide strategy and recorded decisions steer the plans users
+  // create, not the sub-plans built inside other schedules
+  const bool user = hint && hint->user;
+  if (user && strategy == GFFT_KERNEL_AUTO) strategy = g_strategy.load();
   c->prec = prec;
   c->n = n;
   c->device = device;
@@ -367,12 +396,6 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
   GFFT_CUDA(prepare_kernels());
   const bool pow2 = (n & (n - 1)) == 0;
   const int64_t max_single = prec == kC64 ? 16384 : 8192;
-  // A forced strategy (SetKernelStrategy / PlanOptions.Strategy,
-  // internal/planner/selection.go:71-78) picks the schedule class: the
-  // step kernels map to the two-pass schedule, DIT/Stockham to the
-  // single-pass one; a class that cannot serve n falls back to auto.
-  const bool want_twopass = strategy == GFFT_KERNEL_SIXSTEP || strategy == GFFT_KERNEL_EIGHTSTEP;
-  const bool want_single = strategy == GFFT_KERNEL_DIT || strategy == GFFT_KERNEL_STOCKHAM;
   if (strategy == GFFT_KERNEL_AUTO) {
     std::string tok;
     if (wisdom_lookup(n, prec, &tok) && core_init_variant(c, prec, n, device, tok) == GFFT_OK) return GFFT_OK;
@@ -397,7 +420,14 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
     c->n = n;
     c->device = device;
     clear_error();
+    if (user) strategy = recorded_decision(n);  // a recorded class, else the size-class rules
   }
+  // A forced strategy (SetKernelStrategy / PlanOptions.Strategy,
+  // internal/planner/selection.go:71-78) picks the schedule class: the
+  // step kernels map to the two-pass schedule, DIT/Stockham to the
+  // single-pass one; a class that cannot serve n falls back to auto.
+  const bool want_twopass = strategy == GFFT_KERNEL_SIXSTEP || strategy == GFFT_KERNEL_EIGHTSTEP;
+  const bool want_single = strategy == GFFT_KERNEL_DIT || strategy == GFFT_KERNEL_STOCKHAM;
   const bool want_bluestein = strategy == GFFT_KERNEL_BLUESTEIN;
   if (pow2 && n <= max_single && !want_twopass && !want_bluestein) return init_pow2(c, default_ept(prec, n));
   if (pow2 && !want_single && strategy != GFFT_KERNEL_BLUESTEIN) {

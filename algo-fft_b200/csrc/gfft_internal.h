@@ -105,6 +105,7 @@ struct PlanHint {
   int64_t batch = 0;   // transforms per call
   int64_t stride = 1;  // element stride inside one transform
   int real = 0;        // 1: the complex child of a real transform of length 2n
+  bool user = false;   // a plan the user asked for (not a sub-plan of another schedule)
 };
 
 // Chooses and prepares the schedule of a 1-D complex transform of length n:
@@ -113,6 +114,10 @@ struct PlanHint {
 // else defaults.
 gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy = GFFT_KERNEL_AUTO,
                       const PlanHint* hint = nullptr);
+// Process-wide strategy override and per-length strategy decisions.
+void set_kernel_strategy(int s);
+int get_kernel_strategy();
+void record_decision(int64_t n, int s);
 // The learned cost model's choice among variant_tokens(prec, n) for the
 // hinted shape (false when no model is loaded or n has < 2 variants).
 bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* token);

@@ -74,6 +74,7 @@ static gfft_status axis_init(Axis* a, int prec, int64_t n, int64_t inner, int64_
   hint.planner = planner;
   hint.batch = std::max<int64_t>(1, batch) * inner * outer;  // transforms of this axis per call
   hint.stride = inner;
+  hint.user = true;
   gfft_status s = core_init(&a->core, prec, n, device, GFFT_KERNEL_AUTO, &hint);
   if (s != GFFT_OK) return s;
   if (inner > 1 && n > 1 && column_sched(n, prec, &a->cs)) {

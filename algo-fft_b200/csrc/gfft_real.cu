@@ -154,6 +154,7 @@ gfft_status gfft_plan_real_new(gfft_plan_real** out, int32_t precision, int64_t 
   hint.planner = o.planner;
   hint.batch = o.batch;
   hint.real = 1;
+  hint.user = true;
   gfft_status s = core_init(&p->child, precision, p->h, o.device, o.strategy, &hint);
   cudaError_t e = cudaSuccess;
   if (s == GFFT_OK) e = cudaMalloc(&p->wt, size_t(p->h + 1) * elem_bytes(precision));

@@ -103,6 +103,16 @@ GFFT_API void gfft_plan_close(gfft_plan* plan);
  * copy exists for callers that want separately closable handles).  Closing
  * either leaves the other intact. */
 GFFT_API gfft_status gfft_plan_clone(gfft_plan** out, const gfft_plan* src);
+/* SetKernelStrategy / GetKernelStrategy (plan.go:110-120): a process-wide
+ * GFFT_KERNEL_* applied to plans created with GFFT_KERNEL_AUTO;
+ * GFFT_KERNEL_AUTO restores automatic selection. */
+GFFT_API void gfft_set_kernel_strategy(int32_t strategy);
+GFFT_API int32_t gfft_get_kernel_strategy(void);
+/* RecordBenchmarkDecision (plan.go:122-125, internal/planner/
+ * selection.go:42-60): the strategy class automatic selection uses for
+ * length n when the wisdom store, measurement and the learned model have
+ * not decided; only DIT, Stockham, SixStep and EightStep are recorded. */
+GFFT_API void gfft_record_benchmark_decision(int64_t n, int32_t strategy);
 /* NewPlanPooled / NewPlanPooledWithOptions (plan.go:1040-1118): like
  * gfft_plan_new, but gfft_plan_close returns the plan to a process-wide pool
  * keyed by (device, precision, n, planner, strategy) and the next pooled

@@ -120,3 +120,34 @@ def test_planner_helpers_share_options():
     with pl2.Plan2D32(8, 16) as p2, pl2.Plan3D64(4, 4, 4) as p3, pl2.PlanReal(64) as pr, \
             pl2.PlanReal2D(8, 8) as prr, pl2.PlanND32((2, 3, 4)) as pnd:
         assert p2.Len() == 128 and p3.Len() == 64 and pr.Len() == 64 and prr.Len() == 64 and pnd.Len() == 24
+
+
+def test_global_kernel_strategy_and_recorded_decisions():
+    # plan.go:110-125: the process-wide strategy steers plans created with
+    # KernelAuto; recorded per-length decisions apply under auto selection
+    saved = algofft.ExportWisdomToString()
+    algofft.ClearWisdom()
+    try:
+        assert algofft.GetKernelStrategy() == algofft.KernelAuto
+        algofft.SetKernelStrategy(algofft.KernelBluestein)
+        assert algofft.GetKernelStrategy() == algofft.KernelBluestein
+        with algofft.NewPlan(1024) as p:
+            assert "bluestein" in p.Algorithm()  # its inner FFT_M stays a normal plan
+            x = seeded_complex(1024, seed=4)
+            y = np.empty_like(x)
+            p.Forward(y, x)
+            assert rel_l2(y, np.fft.fft(x.astype(np.complex128))) <= tol_c2c(1024, False)
+        algofft.SetKernelStrategy(algofft.KernelAuto)
+        algofft.RecordBenchmarkDecision(8192, algofft.KernelSixStep)
+        algofft.RecordBenchmarkDecision(4096, algofft.KernelBluestein)  # not a recordable class: ignored
+        with algofft.NewPlan(8192) as p:
+            assert "-tp-" in p.Algorithm()
+        with algofft.NewPlan(4096) as p:
+            assert "-p2-" in p.Algorithm()
+        algofft.RecordBenchmarkDecision(8192, algofft.KernelStockham)
+        with algofft.NewPlan(8192) as p:
+            assert "-p2-" in p.Algorithm()
+    finally:
+        algofft.SetKernelStrategy(algofft.KernelAuto)
+        algofft.ClearWisdom()
+        algofft.ImportWisdomFromString(saved)
