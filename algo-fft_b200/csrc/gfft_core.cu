@@ -33,10 +33,19 @@ static std::vector<ThreePassKernel>& threepass_table() {
 void register_pow2(const Pow2Kernel& k) { pow2_table().push_back(k); }
 void register_threepass(const ThreePassKernel& k) { threepass_table().push_back(k); }
 
-const ThreePassKernel* find_threepass(int prec, int64_t n, int dir) {
+const ThreePassKernel* find_threepass(int prec, int64_t n, int dir, int tma, int te, int emax, int nst) {
   for (const auto& k : threepass_table())
-    if (k.prec == prec && int64_t(k.n1) * k.m1 * k.m2 == n && k.dir == dir) return &k;
+    if (k.prec == prec && int64_t(k.n1) * k.m1 * k.m2 == n && k.dir == dir && k.tma == tma &&
+        (tma == 0 || (k.te == te && k.emax == emax && k.nst == nst)))
+      return &k;
   return nullptr;
+}
+
+std::vector<const ThreePassKernel*> threepass_variants(int prec, int64_t n, int dir) {
+  std::vector<const ThreePassKernel*> v;
+  for (const auto& k : threepass_table())
+    if (k.prec == prec && int64_t(k.n1) * k.m1 * k.m2 == n && k.dir == dir) v.push_back(&k);
+  return v;
 }
 void register_twopass(const TwoPassKernel& k) { twopass_table().push_back(k); }
 
@@ -209,6 +218,7 @@ static int default_ept(int prec, int64_t n) {
 }
 
 static std::string twopass_token(const TwoPassKernel* k);
+static std::string threepass_token(const ThreePassKernel* k);
 
 // Two-pass plan: tables W_N1, W_N2 and the split table of W_N in one
 // allocation; slot geometry sized so the live intermediate stays in L2.
@@ -276,15 +286,24 @@ static gfft_status init_threepass(PlanCore* c, const ThreePassKernel* f, const T
   GFFT_CUDA(cudaStreamSynchronize(0));
   c->bt_shift = shn;
   c->btm_shift = shm;
+  GFFT_CUDA(cudaMalloc(&c->status, sizeof(unsigned)));
+  GFFT_CUDA(cudaMemset(c->status, 0, sizeof(unsigned)));
   c->t3[0] = f;
   c->t3[1] = inv;
   c->algo = Algo::ThreePass;
-  c->name = "gpu-sm100-tp3-" + std::to_string(n1) + "x" + std::to_string(m1) + "x" + std::to_string(m2);
+  c->name = threepass_token(f);
   return GFFT_OK;
 }
 
 static std::string pow2_token(int n, int ept) {
   return "gpu-sm100-p2-n" + std::to_string(n) + "-e" + std::to_string(ept);
+}
+
+static std::string threepass_token(const ThreePassKernel* k) {
+  std::string t = std::string(k->tma ? "gpu-sm100-tp3t-" : "gpu-sm100-tp3-") + std::to_string(k->n1) + "x" +
+                  std::to_string(k->m1) + "x" + std::to_string(k->m2);
+  if (k->tma) t += "-t" + std::to_string(k->te) + "-e" + std::to_string(k->emax) + "-s" + std::to_string(k->nst);
+  return t;
 }
 
 static std::string twopass_token(const TwoPassKernel* k) {
@@ -298,8 +317,7 @@ std::vector<std::string> variant_tokens(int prec, int64_t n) {
     if (n <= (prec == kC64 ? 16384 : 8192))
       for (const Pow2Kernel* k : pow2_variants(prec, int(n), -1)) v.push_back(pow2_token(k->n, k->ept));
     for (const TwoPassKernel* k : twopass_variants(prec, n, -1)) v.push_back(twopass_token(k));
-    if (const ThreePassKernel* k = find_threepass(prec, n, -1))
-      v.push_back("gpu-sm100-tp3-" + std::to_string(k->n1) + "x" + std::to_string(k->m1) + "x" + std::to_string(k->m2));
+    for (const ThreePassKernel* k : threepass_variants(prec, n, -1)) v.push_back(threepass_token(k));
   } else if (n > 1 && is_smooth7(n)) {
     // runtime-radix schedules (single CTA when it fits, two passes when n
     // has a 7-smooth divisor >= 2 below sqrt n) against Bluestein
@@ -343,6 +361,13 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     const ThreePassKernel* f = find_threepass(prec, n, -1);
     const ThreePassKernel* i = find_threepass(prec, n, +1);
     if (f && i && f->n1 == a && f->m1 == b && f->m2 == te) return init_threepass(c, f, i);
+  }
+  int m2 = 0, ns = 0;
+  if (std::sscanf(tok.c_str(), "gpu-sm100-tp3t-%dx%dx%d-t%d-e%d-s%d", &a, &b, &m2, &te, &e, &ns) == 6 &&
+      int64_t(a) * b * m2 == n) {
+    const ThreePassKernel* f = find_threepass(prec, n, -1, 1, te, e, ns);
+    const ThreePassKernel* i = find_threepass(prec, n, +1, 1, te, e, ns);
+    if (f && i && f->n1 == a && f->m1 == b && f->m2 == m2) return init_threepass(c, f, i);
   }
   long long ln = 0, l1 = 0, l2 = 0;
   if (std::sscanf(tok.c_str(), "gpu-sm100-mixed-n%lld", &ln) == 1 && ln == n && is_smooth7(n)) return init_generic(c);
@@ -536,6 +561,8 @@ static gfft_status exec_threepass(const PlanCore* c, int dir, void* dst, const v
   p.btm.hi = c->btm_hi;
   p.btm.shift = c->btm_shift;
   p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+  p.status = c->status;
+  p.spin_limit = 1u << 22;
   cudaError_t e = cudaSuccess;
   for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += nb) {
     const int64_t m = std::min(nb, count - b0);

@@ -265,7 +265,7 @@ static bool plan_features(int prec, int64_t n, int64_t batch, int64_t stride, in
   f[7] = float(prec);
   f[8] = float(std::log2(double(std::max<int64_t>(1, stride))));
   f[9] = float(real ? 1 : 0);
-  int a = 0, b = 0, te = 0, e = 0;
+  int a = 0, b = 0, te = 0, e = 0, ns = 0, l = 0;
   long long l1 = 0, l2 = 0, ln = 0;
   if (std::sscanf(tok.c_str(), "gpu-sm100-p2-n%d-e%d", &a, &e) == 2) {
     f[10] = 1.f;
@@ -276,6 +276,10 @@ static bool plan_features(int prec, int64_t n, int64_t batch, int64_t stride, in
     f[15] = float(ilog2f(te));
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-tp3-%dx%dx%d", &a, &b, &te) == 3) {
     f[11] = 1.f;  // a multi-pass schedule with no tile parameters: the three-pass form
+  } else if (std::sscanf(tok.c_str(), "gpu-sm100-tp3t-%dx%dx%d-t%d-e%d-s%d", &a, &b, &l, &te, &e, &ns) == 6) {
+    f[11] = 1.f;  // the TMA-staged three-pass form: its tile and elements per thread
+    f[14] = float(ilog2f(e));
+    f[15] = float(ilog2f(te));
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixed2-%lldx%lld", &l1, &l2) == 2) {
     f[12] = 1.f;
     f[14] = 1.f;

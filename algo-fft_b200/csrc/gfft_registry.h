@@ -39,13 +39,17 @@ struct ThreePassParams;
 struct ThreePassKernel {
   int prec, n1, m1, m2, dir;
   int tpb, smem;
+  int tma = 0, te = 0, emax = 0, nst = 0;  // TMA-staged variant: tile elements, elements per thread, stages
   const void* func[3];  // passes 1..3
   cudaError_t (*launch)(const ThreePassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st);
 };
 
 void register_pow2(const Pow2Kernel& k);
 void register_threepass(const ThreePassKernel& k);
-const ThreePassKernel* find_threepass(int prec, int64_t n, int dir);
+// The plain kernels (tma = 0) unless a TMA-staged variant is named.
+const ThreePassKernel* find_threepass(int prec, int64_t n, int dir, int tma = 0, int te = 0, int emax = 0,
+                                      int nst = 0);
+std::vector<const ThreePassKernel*> threepass_variants(int prec, int64_t n, int dir);
 void register_twopass(const TwoPassKernel& k);
 const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te = 0, int emax = 0);
 std::vector<const TwoPassKernel*> twopass_variants(int prec, int64_t n, int dir);

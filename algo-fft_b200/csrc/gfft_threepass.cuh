@@ -31,6 +31,8 @@ struct ThreePassParams {
   BigTwiddle bt;        // W_N (pass-1 twiddle)
   BigTwiddle btm;       // W_M (pass-2 twiddle)
   double scale;         // applied by pass 3 (1/N for the inverse)
+  unsigned* status;     // set to 1 when a bounded wait of a TMA-staged pass expires
+  unsigned spin_limit;  // try_wait rounds of that wait
 };
 
 template <typename C, int N1, int E1, int C1, int M1, int E2, int C2, int M2, int E3, int C3, int DIR>

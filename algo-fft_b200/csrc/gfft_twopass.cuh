@@ -27,29 +27,55 @@
 #pragma once
 #include "gfft_pow2.cuh"
 #include "gfft_sched.cuh"
+#include "gfft_tma.cuh"
 
 namespace gfft {
 
 // Tile of NC columns of length L, EPT elements per thread.
-template <int L, int EPT, int NC, int ES>
+// DENSE tiles keep rows of exactly NC elements, the layout a TMA tile copy
+// writes; they need rows of at least 128 bytes, so that every warp access of
+// a stage (whole rows) is bank-conflict free.
+template <int L, int EPT, int NC, int ES, bool DENSE = false>
 struct ColShape {
   static_assert((NC & (NC - 1)) == 0, "NC must be a power of two");
+  static_assert(!DENSE || NC * ES >= 128, "dense tiles need rows of at least 128 bytes");
   static constexpr int T = L / EPT;     // threads per column
   static constexpr int TPB = T * NC;    // threads per tile
   // Rows of NC+1 elements when NC >= 16 (odd pitch: row-wise and column-wise
   // accesses are both bank-conflict free); narrower tiles use an XOR swizzle
   // of the column index by the row, which keeps most of that property.
-  static constexpr bool PITCHED = NC >= 16;
+  static constexpr bool PITCHED = !DENSE && NC >= 16;
   static constexpr int PITCH = PITCHED ? NC + 1 : NC;
   static constexpr int SMEM = L * PITCH * ES;
   __device__ static __forceinline__ int phys(int row, int c) {
-    if constexpr (PITCHED) return row * PITCH + c;
+    if constexpr (DENSE) return row * NC + c;
+    else if constexpr (PITCHED) return row * PITCH + c;
     else return row * NC + (c ^ (row & (NC - 1)));
   }
 };
 
-enum { LOAD_STREAM = 0, LOAD_L2 = 1 };
-enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1 };
+// LOAD_SMEM: the tile is already in shared memory (a TMA copy put it there).
+enum { LOAD_STREAM = 0, LOAD_L2 = 1, LOAD_SMEM = 2 };
+// OUT_SMEM: the result, scaled, back into the tile's rows (for a TMA store);
+// OUT_SMEM_TWIDDLE_T: times the big twiddle, transposed into rows of L + 1
+// elements per column, for a coalesced store of whole columns.
+// OUT_SMEM_TWIDDLE_SW: times the big twiddle, transposed into boxes of 128-byte
+// rows in the copy engine's 128-byte swizzle (see swz128), for TMA stores of
+// whole columns.
+enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1, OUT_SMEM = 2, OUT_SMEM_TWIDDLE_T = 3, OUT_SMEM_TWIDDLE_SW = 4 };
+
+// Element (row, c) of a transposed tile held as L / RE boxes of NC rows (one
+// per column c) of 128 bytes (RE elements of consecutive rows), in the
+// layout of a TMA copy with 128-byte swizzle: the 16-byte chunk j of box row
+// c sits at chunk j ^ (c mod 8).  Writes of a warp (whole rows of the
+// untransposed tile) then spread over all banks.  The boxes start on
+// 1024-byte boundaries.
+template <typename C, int NC>
+__device__ __forceinline__ int swz128(int row, int c) {
+  constexpr int RE = 128 / int(sizeof(C)), EPC = 16 / int(sizeof(C));
+  const int k = row % RE;
+  return (row / RE) * (NC * RE) + c * RE + (((k / EPC) ^ (c & 7)) * EPC) + (k % EPC);
+}
 
 template <int LOADK, typename C>
 __device__ __forceinline__ C gload(const C* p) {
@@ -61,14 +87,15 @@ __device__ __forceinline__ C gload(const C* p) {
 // Element (row, c) of the tile lives at sh[phys(row, c)]; global row r of
 // column c is at in[r*ISTRIDE + c].
 // ISTRIDE / OSTRIDE = 0 take the row pitch from `pitch` at run time.
-template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE>
+template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE,
+          bool DENSE = false>
 __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
                                           int t, int c, bool active, const C* __restrict__ tw,
                                           typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2,
                                           int64_t pitch = 0) {
   const int64_t IS = ISTRIDE > 0 ? ISTRIDE : pitch;
   const int64_t OS = OSTRIDE > 0 ? OSTRIDE : pitch;
-  using S = ColShape<L, EPT, NC, sizeof(C)>;
+  using S = ColShape<L, EPT, NC, sizeof(C), DENSE>;
   using SC = Sched<L, EPT>;
   constexpr int T = S::T;
   constexpr int RS = SC::radix_at(P);
@@ -76,9 +103,27 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
   constexpr int STRIDE = L / RS;
   constexpr bool FIRST = (P == 1);
   constexpr bool LAST = (P * RS == L);
+  // the stage read shared memory, so it must sync before writing it
+  constexpr bool READ_SH = !FIRST || LOADK == LOAD_SMEM;
+  constexpr bool BIGTW = LAST && (MODE == OUT_SMEM_TWIDDLE || MODE == OUT_SMEM_TWIDDLE_T || MODE == OUT_SMEM_TWIDDLE_SW);
+
+  // The big twiddles of the last stage are fetched before the stage's own
+  // reads and butterflies, so their latency hides behind that work.
+  // W_N^{n2*(row0 + r*P)} = b * s^r with b = W_N^{n2*row0} (one lookup per
+  // butterfly) and s = W_N^{n2*P} (one per thread); the powers of s come
+  // from a product tree, so no per-element table lookup is scattered across
+  // the warp.
+  [[maybe_unused]] C tw_s{}, tw_b[Q];
+  if constexpr (BIGTW) {
+    if (active) {
+      tw_s = big_twiddle<C, DIR>(bt, n2 * P);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) tw_b[q] = big_twiddle<C, DIR>(bt, n2 * (t + q * T));
+    }
+  }
 
   if (active) {
-    if constexpr (FIRST) {
+    if constexpr (FIRST && LOADK != LOAD_SMEM) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
@@ -94,7 +139,9 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
     for (int q = 0; q < Q; ++q) {
       if constexpr (P > 1) {
         const int k = (t + q * T) & (P - 1);
-        apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + k * (L / (P * RS))));
+        // DENSE (TMA-staged) callers keep the W_L table in shared memory
+        if constexpr (DENSE) apply_twiddles<RS, DIR>(v + q * RS, tw[k * (L / (P * RS))]);
+        else apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + k * (L / (P * RS))));
       }
       dft<RS, DIR>(v + q * RS);
     }
@@ -111,33 +158,43 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
           st_stream(out + int64_t(t + q * T + r * P) * OS + c, o);
         }
     }
-  } else if constexpr (LAST) {
-    if constexpr (!FIRST) __syncthreads();
+  } else if constexpr (LAST && MODE == OUT_SMEM) {
+    if constexpr (READ_SH) __syncthreads();
     if (active) {
-      // W_N^{n2*(row0 + r*P)} = b * s^r with b = W_N^{n2*row0} (one lookup per
-      // butterfly) and s = W_N^{n2*P} (one per thread); the powers of s come
-      // from a product tree, so no per-element table lookup is scattered
-      // across the warp.
-      const C s = big_twiddle<C, DIR>(bt, n2 * P);
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) {
+          C o = v[q * RS + r];
+          if constexpr (DIR > 0) o = cscale(o, scale);
+          sh[S::phys(t + q * T + r * P, c)] = o;
+        }
+    }
+  } else if constexpr (LAST) {
+    if constexpr (READ_SH) __syncthreads();
+    if (active) {
       C pw[RS];
       pw[0] = C{1, 0};
-      if constexpr (RS > 1) pw[1] = s;
+      if constexpr (RS > 1) pw[1] = tw_s;
 #pragma unroll
       for (int r = 2; r < RS; ++r) pw[r] = cmul(pw[r / 2], pw[r - r / 2]);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int row0 = t + q * T;
-        const C b = big_twiddle<C, DIR>(bt, n2 * row0);
+        const C b = tw_b[q];
 #pragma unroll
         for (int r = 0; r < RS; ++r) {
           const C w = r == 0 ? b : cmul(b, pw[r]);
-          sh[S::phys(row0 + r * P, c)] = cmul(v[q * RS + r], w);
+          if constexpr (MODE == OUT_SMEM_TWIDDLE_T) sh[c * (L + 1) + row0 + r * P] = cmul(v[q * RS + r], w);
+          else if constexpr (MODE == OUT_SMEM_TWIDDLE_SW) sh[swz128<C, NC>(row0 + r * P, c)] = cmul(v[q * RS + r], w);
+          else sh[S::phys(row0 + r * P, c)] = cmul(v[q * RS + r], w);
         }
       }
     }
+    if constexpr (DENSE) fence_async_smem();  // the tile may leave by a TMA store
     __syncthreads();
   } else {
-    if constexpr (!FIRST) __syncthreads();
+    if constexpr (READ_SH) __syncthreads();
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
@@ -149,8 +206,8 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
       }
     }
     __syncthreads();
-    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE>(v, in, out, sh, t, c, active, tw, scale,
-                                                                         bt, n2, pitch);
+    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE, DENSE>(v, in, out, sh, t, c, active, tw,
+                                                                                scale, bt, n2, pitch);
   }
 }
 

@@ -51,7 +51,7 @@ TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6,
 def launches_of(algorithm: str, count: int, n: int, es: int) -> int:
     """Kernel launches of one ForwardBatch of this plan (multi-pass plans:
     one launch per pass per chunk of up to 1 GiB of intermediate)."""
-    passes = 3 if "-tp3-" in algorithm else 2 if "-tp-" in algorithm else 1
+    passes = 3 if ("-tp3-" in algorithm or "-tp3t-" in algorithm) else 2 if "-tp-" in algorithm else 1
     if passes > 1:
         chunk = max(1, min(count, (1 << 30) // (n * es)))
         return passes * ((count + chunk - 1) // chunk)
@@ -442,7 +442,9 @@ def main():
     dom_bytes = bytes_per_transform(dom) * bufs[dom][2] / dom_launches  # algorithmic bytes per launch
     peak, peak_kind = peak_hbm()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    if "-tp3-" in dom_alg:
+    if "-tp3t-" in dom_alg:
+        kname = f"k_tp3t (TMA-staged three passes, one persistent launch each; N={dom}, {dom_alg})"
+    elif "-tp3-" in dom_alg:
         kname = f"k_tp3 (three passes, one launch each; N={dom}, {dom_alg})"
     elif "-tp-" in dom_alg:
         kname = f"k_tp_split (two-pass, pass 1 and pass 2 alternate; N={dom}, {dom_alg})"

@@ -283,3 +283,45 @@ def test_three_pass_complex128(n):
     assert rel_l2(y[:n], np.fft.fft(x[:n])) <= tol_c2c(n, True)
     assert rel_l2(back, x) <= 2 * tol_c2c(n, True)
 
+
+
+@pytest.mark.parametrize("n,prec", [(2 ** 21, algofft.COMPLEX64), (2 ** 23, algofft.COMPLEX64),
+                                    (2 ** 21, algofft.COMPLEX128), (2 ** 24, algofft.COMPLEX128)])
+def test_tma_three_pass_variants(n, prec):
+    # the TMA-staged three-pass kernels (persistent, tiles copied by the copy
+    # engine) give the plain three-pass results within the stated tolerance
+    c128 = prec == algofft.COMPLEX128
+    toks = [t for t in algofft.Variants(n, prec) if "-tp3t-" in t]
+    assert len(toks) >= 2
+    count = 3
+    x = seeded_complex(count * n, seed=n % 83, dtype=np.complex128 if c128 else np.complex64)
+    ref = np.fft.fft(x[:n].astype(np.complex128))
+    for tok in toks:
+        with algofft.Plan(n, prec, variant=tok) as p:
+            assert p.Algorithm() == tok
+            y = _run(p, x, count)
+            back = _run(p, y, count, inverse=True)
+            p.Check()
+        assert rel_l2(y[:n], ref) <= tol_c2c(n, c128), tok
+        assert rel_l2(back, x) <= 2 * tol_c2c(n, c128), tok
+
+
+def test_tma_three_pass_unaligned_buffers():
+    # a source and destination 8 bytes off a 16-byte boundary cannot be
+    # addressed by the copy engine: the plan takes the plain kernels
+    import torch
+    n, count = 2 ** 21, 2
+    tok = [t for t in algofft.Variants(n) if "-tp3t-" in t][0]
+    x = seeded_complex(count * n, seed=9)
+    raw = torch.zeros(count * n + 1, dtype=torch.complex64, device="cuda")
+    raw[1:] = torch.from_numpy(x).cuda()
+    out = torch.zeros_like(raw)
+    src, dst = raw[1:], out[1:]
+    assert src.data_ptr() % 16 == 8
+    with algofft.Plan(n, variant=tok) as p:
+        p.ForwardBatch(dst, src, count)
+        torch.cuda.synchronize()
+        p.Check()
+    y = dst.cpu().numpy()
+    assert rel_l2(y[:n], np.fft.fft(x[:n].astype(np.complex128))) <= tol_c2c(n, False)
+    assert rel_l2(y[n:], np.fft.fft(x[n:].astype(np.complex128))) <= tol_c2c(n, False)
