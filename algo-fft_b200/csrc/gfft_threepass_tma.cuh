@@ -4,8 +4,8 @@
 //
 // Each pass is a persistent kernel: CTA b takes tiles b, b + grid, ...  A
 // tile (L rows of NC adjacent columns) arrives in shared memory by one TMA
-// tile copy into one of NST stage buffers; one thread keeps NST - 1 copies
-// in flight ahead of the tile being transformed, so the copy engine streams
+// tile copy into one of NST stage buffers; one thread keeps up to NST - 1
+// copies in flight ahead of the tile being transformed, so the copy engine streams
 // the next tiles while the threads run the Stockham stages in place on the
 // current one (rows of NC elements, the layout the copy writes; whole-row
 // warp accesses keep it bank-conflict free).  Stores:
@@ -121,26 +121,38 @@ k_tp3t(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensor
 
   C v[EPT];
   int64_t j = 0;
-  for (; j < nloc; ++j) {
-    const int s = int(j % NST);
-    C* sh = bufs + s * BUFE;
+  // Refill of the buffer tile j - 1 used, with tile j + NST - 1.  With three
+  // or more stages it comes after tile j's butterflies, when the store that
+  // read that buffer (committed one tile earlier) has long finished; with
+  // two it must come first, or no copy would overlap the butterflies.
+  constexpr bool LATE = NST >= 3;
+  auto refill = [&]() {
     if (tid == 0 && issued < nloc) {
-      // the buffer of tile j - 1: its threads are done (barrier at the end
-      // of the last iteration); its TMA store must have read it too
       bulk_wait_read();
       fence_async_smem();
       issue(issued);
       ++issued;
     }
-    if (!mbar_wait(&bar[s], uint32_t((j / NST) & 1), a.spin_limit)) s_fail = 1;
+  };
+  for (; j < nloc; ++j) {
+    const int s = int(j % NST);
+    C* sh = bufs + s * BUFE;
+    if constexpr (!LATE) refill();
+    // one thread waits for the copy; the barrier passes its completion on
+    // to the others (the copy's writes are ordered before the phase flip
+    // that thread 0 observes, and the barrier orders the rest after it)
+    if (tid == 0 && !mbar_wait(&bar[s], uint32_t((j / NST) & 1), a.spin_limit)) s_fail = 1;
     __syncthreads();
     if (s_fail) break;
     int64_t bl;
     int rowc, col0;
     decode(blockIdx.x + j * gridDim.x, bl, rowc, col0);
+    // every branch ends its butterflies with a fence for the copy engine and
+    // a barrier, so the tile is complete in shared memory before its store
     if constexpr (PASS == 1) {
       col_stage<C, L, EPT, NC, DIR, 1, LOAD_SMEM, OUT_SMEM_TWIDDLE_SW, 1, 1, true>(
           v, nullptr, nullptr, sh, t, c, true, s_tw, Re(1), a.bt, int64_t(col0 + c));
+      if constexpr (LATE) refill();
       if (tid == 0) {  // Y[m][k1]: box i holds rows k1 = i*RE.. of columns m = col0..
         for (int i = 0; i < L / K::RE; ++i) tma_store_3d(&tout, sh + i * NC * K::RE, i * K::RE * W, col0, int(bl));
         bulk_commit();
@@ -148,6 +160,7 @@ k_tp3t(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensor
     } else if constexpr (PASS == 2) {
       col_stage<C, L, EPT, NC, DIR, 1, LOAD_SMEM, OUT_SMEM_TWIDDLE, 1, 1, true>(
           v, nullptr, nullptr, sh, t, c, true, s_tw, Re(1), a.bt, int64_t(rowc));
+      if constexpr (LATE) refill();
       if (tid == 0) {
         tma_store_4d(&tin, sh, col0 * W, rowc, 0, int(bl));  // in place
         bulk_commit();
@@ -157,12 +170,14 @@ k_tp3t(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensor
           v, nullptr, nullptr, sh, t, c, true, s_tw, Re(a.scale), a.bt, 0);
       fence_async_smem();
       __syncthreads();
+      if constexpr (LATE) refill();
       if (tid == 0) {
         tma_store_4d(&tout, sh, col0 * W, rowc, 0, int(bl));
         bulk_commit();
       }
     }
-    __syncthreads();
+    // the early refill of the next iteration reuses this buffer
+    if constexpr (!LATE) __syncthreads();
   }
   if (tid == 0) {
     if (j < nloc) {

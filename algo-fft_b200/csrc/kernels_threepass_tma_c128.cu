@@ -1,5 +1,5 @@
 // TMA-staged three-pass kernels, complex128, N = 2^21..2^24: tiles of 4096
-// and 2048 elements, 4 or 8 elements per thread, two or three stage buffers.
+// and 2048 elements, 8 elements per thread, two or three stage buffers.
 #include "gfft_internal.h"
 #include "kernels_threepass_tma.cuh"
 
@@ -16,7 +16,6 @@ struct RegThreePassTmaC128 {
   RegThreePassTmaC128() {
     reg_shapes<4096, 8, 3>();
     reg_shapes<2048, 8, 3>();
-    reg_shapes<2048, 4, 3>();
     reg_shapes<2048, 8, 2>();
   }
 } reg_threepass_tma_c128;

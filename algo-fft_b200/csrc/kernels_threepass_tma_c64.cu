@@ -1,5 +1,5 @@
 // TMA-staged three-pass kernels, complex64, N = 2^21..2^24: tiles of 8192
-// and 4096 elements, 8 or 16 elements per thread, two or three stage buffers.
+// and 4096 elements, 16 elements per thread, three stage buffers.
 #include "gfft_internal.h"
 #include "kernels_threepass_tma.cuh"
 
@@ -16,7 +16,6 @@ struct RegThreePassTmaC64 {
   RegThreePassTmaC64() {
     reg_shapes<8192, 16, 3>();
     reg_shapes<4096, 16, 3>();
-    reg_shapes<4096, 8, 3>();
   }
 } reg_threepass_tma_c64;
 }  // namespace

@@ -15,7 +15,6 @@ void reg_shapes() {
 struct RegThreePassTmaC64b {
   RegThreePassTmaC64b() {
     reg_shapes<4096, 16, 2>();
-    reg_shapes<8192, 8, 2>();
   }
 } reg_threepass_tma_c64b;
 }  // namespace

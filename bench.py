@@ -43,9 +43,11 @@ WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^4..2^24, 1 GiB batch per
 
 # DRAM bytes per transform (read + write, all passes) of the multi-pass
 # plans, from ncu captures of small batches (profiles/k_tp_split_n16777216.md,
-# profiles/k_tp3_n8388608.md); used to scale `roofline.traffic` to a launch.
+# profiles/k_tp3_n8388608.md, profiles/k_tp3t_n8388608.md); used to scale
+# `roofline.traffic` to a launch.
 TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6,
-                         "gpu-sm100-tp3-256x256x128": 359.4e6}
+                         "gpu-sm100-tp3-256x256x128": 359.4e6,
+                         "gpu-sm100-tp3t-256x256x128-t4096-e16-s3": 363.4e6}
 
 
 def launches_of(algorithm: str, count: int, n: int, es: int) -> int:
