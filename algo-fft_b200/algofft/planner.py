@@ -10,6 +10,7 @@ autotuner) is the fallback and the judge: regret = time of the chosen variant
 / time of the fastest measured one.
 
     python -m algofft.planner collect --count 3500 --out DATA.jsonl   # on a GPU
+    python -m algofft.planner refresh [--data DATA.jsonl] --out NEW.jsonl  # re-time changed shapes
     python -m algofft.planner train --data DATA.jsonl --out MODEL.bin
     python -m algofft.planner report [--data DATA.jsonl] [--model MODEL.bin] [--exercise]
 
@@ -183,6 +184,24 @@ def collect(count: int, seed: int, out: str, iters: int = 3) -> None:
             f.write(json.dumps(measure_shape(s, iters)) + "\n")
             if i % 250 == 0:
                 print(f"{i} shapes, {time.time() - t0:.0f} s", file=sys.stderr, flush=True)
+
+
+def refresh(data: str, out: str, iters: int = 3) -> int:
+    """Re-times the shapes of `data` whose candidate set changed since they
+    were measured (variants added to or removed from the library), keeps the
+    others, and writes the records to `out` in the same order."""
+    import gzip
+    recs = load_records(data)
+    n_new = 0
+    opener = gzip.open if out.endswith(".gz") else open
+    with opener(out, "wt") as f:
+        for r in recs:
+            if set(r["times"]) != set(Variants(r["n"], r["prec"])):
+                s = {k: r[k] for k in ("prec", "n", "batch", "real")}
+                r = measure_shape(s, iters)
+                n_new += 1
+            f.write(json.dumps(r) + "\n")
+    return n_new
 
 
 DEFAULT_DATA = os.path.join(HERE, "wisdom", "planner_data.jsonl.gz")
@@ -365,6 +384,10 @@ def main(argv=None) -> int:
     c.add_argument("--seed", type=int, default=2024)
     c.add_argument("--iters", type=int, default=3)
     c.add_argument("--out", required=True)
+    f = sub.add_parser("refresh")
+    f.add_argument("--data", default=DEFAULT_DATA)
+    f.add_argument("--iters", type=int, default=3)
+    f.add_argument("--out", required=True)
     t = sub.add_parser("train")
     t.add_argument("--data", required=True)
     t.add_argument("--out", default=DEFAULT_MODEL)
@@ -377,6 +400,8 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     if a.cmd == "collect":
         collect(a.count, a.seed, a.out, a.iters)
+    elif a.cmd == "refresh":
+        print(f"re-timed {refresh(a.data, a.out, a.iters)} shapes", file=sys.stderr)
     elif a.cmd == "train":
         tr, _ = split(load_records(a.data))
         X, y, _, _ = design(tr)
