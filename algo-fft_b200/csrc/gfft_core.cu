@@ -525,6 +525,8 @@ static gfft_status exec_twopass(const PlanCore* c, int dir, void* dst, const voi
   p.bt.hi = c->bt_hi;
   p.bt.shift = c->bt_shift;
   p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+  p.status = c->status;
+  p.spin_limit = 1u << 22;
   cudaError_t e = cudaSuccess;
   for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += nb) {
     const int64_t m = std::min(nb, count - b0);

@@ -277,8 +277,10 @@ static bool plan_features(int prec, int64_t n, int64_t batch, int64_t stride, in
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-tp3-%dx%dx%d", &a, &b, &te) == 3) {
     f[11] = 1.f;  // a multi-pass schedule with no tile parameters: the three-pass form
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-tp3t-%dx%dx%d-t%d-e%d-s%d", &a, &b, &l, &te, &e, &ns) == 6) {
-    f[11] = 1.f;  // the TMA-staged three-pass form: its tile and elements per thread
-    f[14] = float(ilog2f(e));
+    // the TMA-staged three-pass form: tile and elements per thread, the
+    // latter offset by 4 so that it never coincides with a plain tile
+    f[11] = 1.f;
+    f[14] = float(ilog2f(e) + 4);
     f[15] = float(ilog2f(te));
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixed2-%lldx%lld", &l1, &l2) == 2) {
     f[12] = 1.f;

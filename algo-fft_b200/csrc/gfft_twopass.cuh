@@ -33,12 +33,13 @@ namespace gfft {
 
 // Tile of NC columns of length L, EPT elements per thread.
 // DENSE tiles keep rows of exactly NC elements, the layout a TMA tile copy
-// writes; they need rows of at least 128 bytes, so that every warp access of
-// a stage (whole rows) is bank-conflict free.
+// writes.  With rows of 128 bytes or more every warp access of a stage
+// (whole rows) is bank-conflict free; with 64-byte rows the first stage's
+// scattered writes can take twice the minimum wavefronts.
 template <int L, int EPT, int NC, int ES, bool DENSE = false>
 struct ColShape {
   static_assert((NC & (NC - 1)) == 0, "NC must be a power of two");
-  static_assert(!DENSE || NC * ES >= 128, "dense tiles need rows of at least 128 bytes");
+  static_assert(!DENSE || NC * ES >= 64, "dense tiles need rows of at least 64 bytes");
   static constexpr int T = L / EPT;     // threads per column
   static constexpr int TPB = T * NC;    // threads per tile
   // Rows of NC+1 elements when NC >= 16 (odd pitch: row-wise and column-wise
@@ -252,9 +253,15 @@ struct TwoPass {
   static constexpr int TPB = S1::TPB > S2::TPB ? S1::TPB : S2::TPB;
   static constexpr int SMEM = S1::SMEM > S2::SMEM ? S1::SMEM : S2::SMEM;
   static constexpr int EPT = EPT1 > EPT2 ? EPT1 : EPT2;
-  // resident CTAs per SM the register allocation must allow (smem-bound)
+  // resident CTAs per SM the register allocation must allow: as many as
+  // the shared memory admits, but never so many that a thread gets fewer
+  // registers than its elements need plus 32 (at least 64; below that the
+  // stages spill)
   static constexpr int MB0 = (200 * 1024) / (SMEM > 0 ? SMEM : 1);
-  static constexpr int MIN_BLOCKS = MB0 < 1 ? 1 : (MB0 > 4 ? 4 : MB0);
+  static constexpr int REGS = EPT * int(sizeof(C)) / 4 + 32 > 64 ? EPT * int(sizeof(C)) / 4 + 32 : 64;
+  static constexpr int MB_REG = 65536 / (TPB * REGS) < 1 ? 1 : 65536 / (TPB * REGS);
+  static constexpr int MB1 = MB0 < MB_REG ? MB0 : MB_REG;
+  static constexpr int MIN_BLOCKS = MB1 < 1 ? 1 : (MB1 > 4 ? 4 : MB1);
 };
 
 // Tile order decode (see the header comment).

@@ -1,7 +1,7 @@
 // TMA-staged three-pass kernels, complex128, N = 2^21..2^24: tiles of 4096
 // and 2048 elements, 8 elements per thread, two or three stage buffers.
 #include "gfft_internal.h"
-#include "kernels_threepass_tma.cuh"
+#include "kernels_cols_tma.cuh"
 
 namespace gfft {
 namespace {

@@ -1,7 +1,7 @@
 // TMA-staged three-pass kernels, complex64, N = 2^21..2^24: tiles of 8192
 // and 4096 elements, 16 elements per thread, three stage buffers.
 #include "gfft_internal.h"
-#include "kernels_threepass_tma.cuh"
+#include "kernels_cols_tma.cuh"
 
 namespace gfft {
 namespace {

@@ -1,7 +1,7 @@
 // TMA-staged three-pass kernels, complex64: shallower pipelines (two stage
 // buffers, more CTAs per SM).
 #include "gfft_internal.h"
-#include "kernels_threepass_tma.cuh"
+#include "kernels_cols_tma.cuh"
 
 namespace gfft {
 namespace {

@@ -289,7 +289,7 @@ def test_three_pass_complex128(n):
                                     (2 ** 21, algofft.COMPLEX128), (2 ** 24, algofft.COMPLEX128)])
 def test_tma_three_pass_variants(n, prec):
     # the TMA-staged three-pass kernels (persistent, tiles copied by the copy
-    # engine) give the plain three-pass results within the stated tolerance
+    # engine) give the FP64 results within the stated tolerance
     c128 = prec == algofft.COMPLEX128
     toks = [t for t in algofft.Variants(n, prec) if "-tp3t-" in t]
     assert len(toks) >= 2
