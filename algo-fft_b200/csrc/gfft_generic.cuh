@@ -3,9 +3,13 @@
 // N = product of radices from {2, 3, 4, 5, 7, 8, 16}, chosen on the host;
 // every stage is Stockham's self-sorting step (see gfft_pow2.cuh) with a
 // runtime radix dispatched to the in-register DFT codelets.  A transform's
-// data sit in shared memory (padded one element every 32) for all stages;
-// T threads own it, each thread holding up to QM butterflies of a stage in
-// registers so a stage can read all its inputs before any thread writes.
+// data sit in shared memory (padded one element every 32) in two buffers:
+// each stage reads one and writes the other, so a thread finishes one
+// butterfly (R values in registers) before it loads the next, and a stage
+// needs one barrier.  T threads own a transform and loop over its
+// butterflies.  (Holding all of a thread's butterflies of a stage in
+// registers, to work in one buffer, spilled to local memory at every
+// launch bound, and the spills reached HBM.)
 //
 // Replaces the reference's 2/3/4/5 mixed-radix recursion
 // (internal/fft/mixedradix.go:45-420) and extends it with radix 7, which the
@@ -20,7 +24,8 @@ struct GenSched {
   int nst;        // number of stages
   int T;          // threads per transform
   int B;          // transforms per CTA
-  int stride;     // shared-memory elements reserved per transform
+  int stride;     // shared-memory elements reserved per transform (both buffers)
+  int half;       // offset of the second buffer within a transform's region
   int radix[20];  // radix of stage s
   int p[20];      // product of the radices before stage s
 };
@@ -31,57 +36,48 @@ __device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
 // butterfly index it yields is past the end of every stage.
 constexpr int kIdleThread = 1 << 28;
 
-// Butterflies a thread may hold in one stage of radix R (R*QM <= 32).
-template <int R>
-struct GenQ {
-  static constexpr int QM = R == 2 ? 16 : R == 3 ? 10 : R == 4 ? 8 : R == 5 ? 6 : R == 7 ? 4 : R == 8 ? 4 : 2;
-};
-
+// One stage: butterflies i = t, t + T, ... of radix R from `in` to `out`.
 template <int R, int DIR, typename C>
-__device__ __forceinline__ void gen_stage(C* x, int n, int p, int T, int t, const C* __restrict__ tw) {
-  constexpr int QM = GenQ<R>::QM;
+__device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, int T, int t,
+                                          const C* __restrict__ tw) {
   const int nb = n / R;
-  C v[QM][R];
-#pragma unroll
-  for (int q = 0; q < QM; ++q) {
-    const int i = t + q * T;
-    if (i < nb) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[q][r] = x[gpad(i + r * nb)];
-    }
-  }
-  __syncthreads();
   const int step = n / (p * R);
+  for (int i = t; i < nb; i += T) {
+    C v[R];
 #pragma unroll
-  for (int q = 0; q < QM; ++q) {
-    const int i = t + q * T;
-    if (i < nb) {
-      const int k = i % p;
-      if (p > 1) apply_twiddles<R, DIR>(v[q], __ldg(tw + k * step));
-      dft<R, DIR>(v[q]);
-      const int j = (i - k) * R + k;
+    for (int r = 0; r < R; ++r) v[r] = in[gpad(i + r * nb)];
+    const int k = i % p;
+    if (p > 1) apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
+    dft<R, DIR>(v);
+    const int j = (i - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[gpad(j + r * p)] = v[q][r];
-    }
+    for (int r = 0; r < R; ++r) out[gpad(j + r * p)] = v[r];
   }
-  __syncthreads();
 }
 
-// Runs all stages on x (shared memory, padded layout) for one direction.
+// Runs all stages for one direction, the data starting in `a` (shared
+// memory, padded layout; the caller synchronises after filling it), `b`
+// the other buffer.  Returns the buffer that holds the result, after a
+// barrier.
 template <int DIR, typename C>
-__device__ __forceinline__ void gen_fft(C* x, const GenSched& s, int t, const C* __restrict__ tw) {
+__device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, const C* __restrict__ tw) {
   for (int st = 0; st < s.nst; ++st) {
     const int p = s.p[st];
     switch (s.radix[st]) {
-      case 2: gen_stage<2, DIR>(x, s.n, p, s.T, t, tw); break;
-      case 3: gen_stage<3, DIR>(x, s.n, p, s.T, t, tw); break;
-      case 4: gen_stage<4, DIR>(x, s.n, p, s.T, t, tw); break;
-      case 5: gen_stage<5, DIR>(x, s.n, p, s.T, t, tw); break;
-      case 7: gen_stage<7, DIR>(x, s.n, p, s.T, t, tw); break;
-      case 8: gen_stage<8, DIR>(x, s.n, p, s.T, t, tw); break;
-      default: gen_stage<16, DIR>(x, s.n, p, s.T, t, tw); break;
+      case 2: gen_stage<2, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 3: gen_stage<3, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 4: gen_stage<4, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 5: gen_stage<5, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 7: gen_stage<7, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 8: gen_stage<8, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      default: gen_stage<16, DIR>(a, b, s.n, p, s.T, t, tw); break;
     }
+    __syncthreads();
+    C* tmp = a;
+    a = b;
+    b = tmp;
   }
+  return a;
 }
 
 // Batched C2C with a runtime schedule: B transforms per CTA, T threads each.
@@ -99,11 +95,11 @@ __global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t 
   if (slot < s.B)
     for (int e = t; e < s.n; e += s.T) x[gpad(e)] = valid ? ld_stream(in + e) : C{0, 0};
   __syncthreads();
-  gen_fft<DIR>(x, s, slot < s.B ? t : kIdleThread, tw);
+  const C* res = gen_fft<DIR>(x, x + s.half, s, slot < s.B ? t : kIdleThread, tw);
   if (valid) {
     C* out = dst + b * odist;
     for (int e = t; e < s.n; e += s.T) {
-      C y = x[gpad(e)];
+      C y = res[gpad(e)];
       if constexpr (DIR > 0) y = cscale(y, scale);
       st_stream(out + e, y);
     }
@@ -155,7 +151,10 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
   }
   __syncthreads();
   const int slot = tid / s.T, t = tid % s.T;
-  gen_fft<DIR>(base + (slot < NC ? slot : 0) * s.stride, s, slot < NC ? t : kIdleThread, tw);
+  C* col = base + (slot < NC ? slot : 0) * s.stride;
+  gen_fft<DIR>(col, col + s.half, s, slot < NC ? t : kIdleThread, tw);
+  // every column's result sits in the same buffer of its region
+  const C* res = base + ((s.nst & 1) ? s.half : 0);
   if (!valid) return;
   if constexpr (MODE == GEN_PASS1) {
     const C* lo = static_cast<const C*>(bt.lo);
@@ -168,13 +167,13 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
       const int64_t m = n2 * k1;
       C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
       if constexpr (DIR > 0) w.y = -w.y;
-      __stcg(out + n2 * L + k1, cmul(base[c * s.stride + gpad(k1)], w));
+      __stcg(out + n2 * L + k1, cmul(res[c * s.stride + gpad(k1)], w));
     }
   } else {
     for (int e = tid; e < L * NC; e += nthr) {
       const int k2 = e / NC, c = e % NC;
       if (col0 + c >= ncols) continue;
-      C v = base[c * s.stride + gpad(k2)];
+      C v = res[c * s.stride + gpad(k2)];
       if constexpr (DIR > 0) v = cscale(v, scale);
       st_stream(out + int64_t(k2) * pitch + col0 + c, v);
     }

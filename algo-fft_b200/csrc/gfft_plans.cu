@@ -20,7 +20,9 @@ static bool smooth7(int64_t n) {
 
 bool is_smooth7(int64_t n) { return smooth7(n); }
 
-static int qm_of(int r) { return r == 2 ? 16 : r == 3 ? 10 : r == 4 ? 8 : r == 5 ? 6 : r == 7 ? 4 : r == 8 ? 4 : 2; }
+// Butterflies of radix r a thread is sized for in one stage (about 16
+// elements); the threads of a transform loop past that when capped at 1024.
+static int qm_of(int r) { return std::max(1, 16 / r); }
 
 // Radix order: 16s, then the rest of the twos (8, 4, 2), then 7s, 5s, 3s.
 static bool make_sched(int64_t n, GenSched* s) {
@@ -56,11 +58,14 @@ static bool make_sched(int64_t n, GenSched* s) {
     T = std::max<int64_t>(T, (n / rad[i] + qm_of(rad[i]) - 1) / qm_of(rad[i]));
   }
   if (T > 32) T = (T + 31) / 32 * 32;
-  if (T > 1024) return false;
+  if (T > 1024) T = 1024;
   s->T = int(T);
-  int stride = int(n - 1 + ((n - 1) >> 5) + 1);
-  if (stride % 2 == 0) ++stride;
-  s->stride = stride;
+  // two padded buffers per transform, an odd total (column-major tiles of
+  // k_gen_cols stay bank-conflict free)
+  const int64_t half = n - 1 + ((n - 1) >> 5) + 1;
+  if (2 * half + 1 > (int64_t(1) << 30)) return false;
+  s->half = int(half);
+  s->stride = int(2 * half + 1);
   s->B = 1;
   return true;
 }

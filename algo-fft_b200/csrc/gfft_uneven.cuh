@@ -64,10 +64,10 @@ __global__ void __launch_bounds__(1024) k_uneven(const C* src, C* dst, const Une
     if (!d.bluestein) {
       for (int e = tid; e < L; e += nthr) x[gpad(e)] = ld_stream(in + e);
       __syncthreads();
-      gen_fft<DIR>(x, d.s, t, W);
+      const C* res = gen_fft<DIR>(x, x + d.s.half, d.s, t, W);
       const Re sc = Re(1.0 / double(L));
       for (int e = tid; e < L; e += nthr) {
-        C y = x[gpad(e)];
+        C y = res[gpad(e)];
         if constexpr (DIR > 0) y = cscale(y, sc);
         st_stream(out + e, y);
       }
@@ -78,17 +78,18 @@ __global__ void __launch_bounds__(1024) k_uneven(const C* src, C* dst, const Une
       for (int e = tid; e < L; e += nthr)
         x[gpad(e)] = e < n ? cmul(ld_stream(in + e), chirp_dir<DIR>(__ldg(ch + e))) : C{0, 0};
       __syncthreads();
-      gen_fft<-1>(x, d.s, t, W);
+      C* y = gen_fft<-1>(x, x + d.s.half, d.s, t, W);
+      C* other = y == x ? x + d.s.half : x;
       // the inverse filter is FFT_M(conj b) = conj(F[(M - k) mod M])
       for (int e = tid; e < L; e += nthr) {
         const C f = DIR < 0 ? __ldg(F + e) : cconj(__ldg(F + (e == 0 ? 0 : L - e)));
-        x[gpad(e)] = cmul(x[gpad(e)], f);
+        y[gpad(e)] = cmul(y[gpad(e)], f);
       }
       __syncthreads();
-      gen_fft<+1>(x, d.s, t, W);
+      const C* res = gen_fft<+1>(y, other, d.s, t, W);
       const Re sc = Re(DIR > 0 ? 1.0 / (double(L) * double(n)) : 1.0 / double(L));
       for (int e = tid; e < n; e += nthr)
-        st_stream(out + e, cscale(cmul(x[gpad(e)], chirp_dir<DIR>(__ldg(ch + e))), sc));
+        st_stream(out + e, cscale(cmul(res[gpad(e)], chirp_dir<DIR>(__ldg(ch + e))), sc));
     }
   }
 }
