@@ -28,6 +28,7 @@ struct GenSched {
   int half;       // offset of the second buffer within a transform's region
   int radix[20];  // radix of stage s
   int p[20];      // product of the radices before stage s
+  float pinv[20]; // 1 / p[s], for the quotient i / p without an integer divide
 };
 
 __device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
@@ -37,8 +38,23 @@ __device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
 constexpr int kIdleThread = 1 << 28;
 
 // One stage: butterflies i = t, t + T, ... of radix R from `in` to `out`.
+// i / p by a float reciprocal (exact for i < 2^24 once corrected by one
+// step either way), then k = i mod p.
+__device__ __forceinline__ int gen_mod(int i, int p, float pinv, int& q) {
+  q = __float2int_rz(__int2float_rn(i) * pinv);
+  int k = i - q * p;
+  if (k < 0) {
+    k += p;
+    --q;
+  } else if (k >= p) {
+    k -= p;
+    ++q;
+  }
+  return k;
+}
+
 template <int R, int DIR, typename C>
-__device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, int T, int t,
+__device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, float pinv, int T, int t,
                                           const C* __restrict__ tw) {
   const int nb = n / R;
   const int step = n / (p * R);
@@ -46,10 +62,11 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, int
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[gpad(i + r * nb)];
-    const int k = i % p;
+    int q;
+    const int k = gen_mod(i, p, pinv, q);
     if (p > 1) apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
     dft<R, DIR>(v);
-    const int j = (i - k) * R + k;
+    const int j = q * p * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) out[gpad(j + r * p)] = v[r];
   }
@@ -63,14 +80,15 @@ template <int DIR, typename C>
 __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, const C* __restrict__ tw) {
   for (int st = 0; st < s.nst; ++st) {
     const int p = s.p[st];
+    const float pi = s.pinv[st];
     switch (s.radix[st]) {
-      case 2: gen_stage<2, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      case 3: gen_stage<3, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      case 4: gen_stage<4, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      case 5: gen_stage<5, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      case 7: gen_stage<7, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      case 8: gen_stage<8, DIR>(a, b, s.n, p, s.T, t, tw); break;
-      default: gen_stage<16, DIR>(a, b, s.n, p, s.T, t, tw); break;
+      case 2: gen_stage<2, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 3: gen_stage<3, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 4: gen_stage<4, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 5: gen_stage<5, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 7: gen_stage<7, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 8: gen_stage<8, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      default: gen_stage<16, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
     }
     __syncthreads();
     C* tmp = a;
@@ -82,11 +100,25 @@ __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, cons
 
 // Batched C2C with a runtime schedule: B transforms per CTA, T threads each.
 // Every thread of the CTA reaches every barrier (idle slots included).
+// With ahead > 0 each CTA first asks the copy engine to bring the input of
+// CTA blockIdx + ahead into L2 (ahead = the co-resident CTAs), so loads
+// find it there about one CTA lifetime later.
 template <typename C, int DIR>
 __global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t count, int64_t idist,
                                                   int64_t odist, const C* __restrict__ tw, GenSched s,
-                                                  typename RealOf<C>::type scale) {
+                                                  typename RealOf<C>::type scale, int64_t ahead) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (ahead > 0) {
+    const int64_t b2 = (int64_t(blockIdx.x) + ahead) * s.B;
+    if (b2 < count) {
+      const int64_t nb = count - b2 < s.B ? count - b2 : s.B;
+      const int64_t bytes = int64_t(s.n) * int64_t(sizeof(C));
+      if (idist == s.n)
+        prefetch_range(src + b2 * idist, nb * bytes, threadIdx.x, blockDim.x);
+      else
+        for (int64_t j = 0; j < nb; ++j) prefetch_range(src + (b2 + j) * idist, bytes, threadIdx.x, blockDim.x);
+    }
+  }
   const int slot = threadIdx.x / s.T, t = threadIdx.x % s.T;
   C* x = reinterpret_cast<C*>(smem_raw) + slot * s.stride;
   const int64_t b = int64_t(blockIdx.x) * s.B + slot;

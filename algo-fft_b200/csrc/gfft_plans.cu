@@ -54,6 +54,7 @@ static bool make_sched(int64_t n, GenSched* s) {
   for (int i = 0; i < s->nst; ++i) {
     s->radix[i] = rad[i];
     s->p[i] = int(prod);
+    s->pinv[i] = float(1.0 / double(prod));
     prod *= rad[i];
     T = std::max<int64_t>(T, (n / rad[i] + qm_of(rad[i]) - 1) / qm_of(rad[i]));
   }
@@ -84,12 +85,22 @@ static cudaError_t launch_generic(const PlanCore* c, int dir, const void* src, v
   const int64_t blocks = (count + s.B - 1) / s.B;
   const size_t smem = size_t(s.B) * s.stride * sizeof(C);
   const Re scale = Re(1.0 / double(c->n));
+  // co-resident CTAs: the L2 prefetch distance (none for a single wave)
+  int dev = 0, sms = 0, occ = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, &k_generic<C, -1>, s.B * s.T, smem);
+  cudaGetLastError();
+  const int64_t resident = int64_t(sms) * std::max(occ, 1);
+  const int64_t ahead = blocks > resident ? resident : 0;
   if (dir < 0)
     k_generic<C, -1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
-                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale);
+                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale,
+                                                                  ahead);
   else
     k_generic<C, +1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
-                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale);
+                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale,
+                                                                  ahead);
   return cudaGetLastError();
 }
 
