@@ -1,6 +1,7 @@
 """Writes gfft_constants.cuh: cos/sin(2*pi*j/R) for the in-register DFT
 codelets (R = 64 covers every power-of-two radix up to 64; 3, 5 and 7 for the
-odd radices), evaluated with mpmath cospi/sinpi at 40 digits and rounded to double."""
+odd radices; 9 for the composite radix 3 x 3), evaluated with mpmath
+cospi/sinpi at 40 digits and rounded to double."""
 import os
 import mpmath
 
@@ -18,7 +19,7 @@ def table(name, r, fn):
 
 
 out = ["// Generated by gen_constants.py; do not edit.\n#pragma once\n\nnamespace gfft {\n"]
-for r in (64, 3, 5, 7):
+for r in (64, 3, 5, 7, 9):
     out.append(table(f"kCos{r}", r, mpmath.cospi))
     out.append(table(f"kSin{r}", r, mpmath.sinpi))
 out.append("}  // namespace gfft\n")

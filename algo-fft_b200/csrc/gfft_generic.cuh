@@ -1,6 +1,6 @@
 // Runtime-schedule Stockham for any 7-smooth length (K3).
 //
-// N = product of radices from {2, 3, 4, 5, 7, 8, 16}, chosen on the host;
+// N = product of radices from {2, 3, 4, 5, 7, 8, 9, 16}, chosen on the host;
 // every stage is Stockham's self-sorting step (see gfft_pow2.cuh) with a
 // runtime radix dispatched to the in-register DFT codelets.  A transform's
 // data sit in shared memory (padded one element every 32) in two buffers:
@@ -88,6 +88,7 @@ __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, cons
       case 5: gen_stage<5, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
       case 7: gen_stage<7, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
       case 8: gen_stage<8, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
+      case 9: gen_stage<9, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
       default: gen_stage<16, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
     }
     __syncthreads();

@@ -43,8 +43,12 @@ template <int R, int M, int DIR, typename C> __device__ __forceinline__ C twc(C 
   else if constexpr (2 * m == R) return C{-a.x, -a.y};
   else if constexpr (4 * m == R) return mul_di<DIR>(a);
   else if constexpr (4 * m == 3 * R) return mul_di<-DIR>(a);
-  else {
-    static_assert(64 % R == 0, "constant roots cover R | 64");
+  else if constexpr (R == 9) {
+    constexpr double c = kCos9[m];
+    constexpr double s = DIR * kSin9[m];
+    return C{Re(c) * a.x - Re(s) * a.y, Re(c) * a.y + Re(s) * a.x};
+  } else {
+    static_assert(64 % R == 0, "constant roots cover R | 64 and R = 9");
     constexpr double c = kCos64[m * (64 / R)];
     constexpr double s = DIR * kSin64[m * (64 / R)];
     return C{Re(c) * a.x - Re(s) * a.y, Re(c) * a.y + Re(s) * a.x};
@@ -113,9 +117,9 @@ __device__ __forceinline__ void twiddle_block(C* a) {
   }
 }
 
-// In-register DFT of R points, natural order in and out.  Powers of two are
-// split R = R1 * R2 (n = R2 n1 + n2, k = k1 + R1 k2): R2 DFTs of size R1,
-// constant twiddles W_R^{n2 k1}, R1 DFTs of size R2.
+// In-register DFT of R points, natural order in and out.  Powers of two and
+// 9 are split R = R1 * R2 (n = R2 n1 + n2, k = k1 + R1 k2): R2 DFTs of size
+// R1, constant twiddles W_R^{n2 k1}, R1 DFTs of size R2.
 template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) {
   if constexpr (R == 1) {
   } else if constexpr (R == 2) {
@@ -132,8 +136,8 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) 
   } else if constexpr (R == 3 || R == 5 || R == 7) {
     dft_odd<R, DIR>(v);
   } else {
-    static_assert(R == 8 || R == 16 || R == 32 || R == 64, "unsupported radix");
-    constexpr int R1 = (R == 8) ? 2 : 4;
+    static_assert(R == 8 || R == 9 || R == 16 || R == 32 || R == 64, "unsupported radix");
+    constexpr int R1 = (R == 8) ? 2 : (R == 9) ? 3 : 4;
     constexpr int R2 = R / R1;
     C a[R];
 #pragma unroll
@@ -176,13 +180,14 @@ __device__ __forceinline__ void apply_twiddles(C* v, C w1) {
 #pragma unroll
       for (int r = 1; r < RS; ++r) v[r] = cmul(v[r], w[r]);
     } else {
-      C lo[8], hi[RS / 8];
+      constexpr int NH = (RS + 7) / 8;  // w^0, w^8, ... up to w^{8 (NH - 1)}
+      C lo[8], hi[NH];
       lo[1] = w1;
 #pragma unroll
       for (int r = 2; r < 8; ++r) lo[r] = cmul(lo[r / 2], lo[r - r / 2]);
       hi[1] = cmul(lo[4], lo[4]);
 #pragma unroll
-      for (int h = 2; h < RS / 8; ++h) hi[h] = cmul(hi[h / 2], hi[h - h / 2]);
+      for (int h = 2; h < NH; ++h) hi[h] = cmul(hi[h / 2], hi[h - h / 2]);
 #pragma unroll
       for (int r = 1; r < RS; ++r) {
         const int a = r % 8, b = r / 8;

@@ -24,7 +24,8 @@ bool is_smooth7(int64_t n) { return smooth7(n); }
 // elements); the threads of a transform loop past that when capped at 1024.
 static int qm_of(int r) { return std::max(1, 16 / r); }
 
-// Radix order: 16s, then the rest of the twos (8, 4, 2), then 7s, 5s, 3s.
+// Radix order: 16s, then the rest of the twos (8, 4, 2), then 7s, 5s, 9s
+// (pairs of threes) and a last 3.
 static bool make_sched(int64_t n, GenSched* s) {
   *s = GenSched{};
   if (n < 2 || n > (int64_t(1) << 30) || !smooth7(n)) return false;
@@ -42,11 +43,19 @@ static bool make_sched(int64_t n, GenSched* s) {
   if (e2 == 3) rad.push_back(8);
   if (e2 == 2) rad.push_back(4);
   if (e2 == 1) rad.push_back(2);
-  for (int p : {7, 5, 3})
+  for (int p : {7, 5})
     while (m % p == 0) {
       rad.push_back(p);
       m /= p;
     }
+  while (m % 9 == 0) {  // pairs of threes as one radix-9 stage
+    rad.push_back(9);
+    m /= 9;
+  }
+  if (m % 3 == 0) {
+    rad.push_back(3);
+    m /= 3;
+  }
   if (int(rad.size()) > 20) return false;
   s->n = int(n);
   s->nst = int(rad.size());

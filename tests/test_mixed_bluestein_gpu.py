@@ -52,7 +52,7 @@ def test_mixed_radix_c64(n):
     assert rel_l2(back, x) <= 2 * tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n", [3, 12, 343, 6000, 50421])
+@pytest.mark.parametrize("n", [3, 9, 12, 81, 343, 2187, 6000, 50421])
 def test_mixed_radix_c128(n):
     count = 3
     x = seeded_complex(n * count, seed=n, dtype=np.complex128)
