@@ -37,7 +37,6 @@ __device__ __forceinline__ int gpad(int e) { return e + (e >> 5); }
 // butterfly index it yields is past the end of every stage.
 constexpr int kIdleThread = 1 << 28;
 
-// One stage: butterflies i = t, t + T, ... of radix R from `in` to `out`.
 // i / p by a float reciprocal (exact for i < 2^24 once corrected by one
 // step either way), then k = i mod p.
 __device__ __forceinline__ int gen_mod(int i, int p, float pinv, int& q) {
@@ -53,22 +52,51 @@ __device__ __forceinline__ int gen_mod(int i, int p, float pinv, int& q) {
   return k;
 }
 
+// One stage: butterflies i = t, t + T, ... of radix R from `in` to `out`
+// (shared memory, padded).  When set, `gin` replaces `in` by the
+// transform's global input (first stage) and `gout` replaces `out` by its
+// global output (last stage, scaled for the inverse); consecutive threads
+// touch consecutive elements of both.
 template <int R, int DIR, typename C>
-__device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, float pinv, int T, int t,
-                                          const C* __restrict__ tw) {
+__device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* gout, typename RealOf<C>::type scale,
+                                          int n, int p, float pinv, int T, int t, const C* __restrict__ tw) {
   const int nb = n / R;
   const int step = n / (p * R);
   for (int i = t; i < nb; i += T) {
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = in[gpad(i + r * nb)];
+    for (int r = 0; r < R; ++r) v[r] = gin ? ld_stream(gin + i + r * nb) : in[gpad(i + r * nb)];
     int q;
     const int k = gen_mod(i, p, pinv, q);
     if (p > 1) apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
     dft<R, DIR>(v);
     const int j = q * p * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) out[gpad(j + r * p)] = v[r];
+    for (int r = 0; r < R; ++r) {
+      if (gout) {
+        C o = v[r];
+        if constexpr (DIR > 0) o = cscale(o, scale);
+        st_stream(gout + j + r * p, o);
+      } else {
+        out[gpad(j + r * p)] = v[r];
+      }
+    }
+  }
+}
+
+template <int DIR, typename C>
+__device__ __forceinline__ void gen_stage_any(int radix, const C* a, C* b, const C* gin, C* gout,
+                                              typename RealOf<C>::type scale, int n, int p, float pi, int T, int t,
+                                              const C* __restrict__ tw) {
+  switch (radix) {
+    case 2: gen_stage<2, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 3: gen_stage<3, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 4: gen_stage<4, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 5: gen_stage<5, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 7: gen_stage<7, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 8: gen_stage<8, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 9: gen_stage<9, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    default: gen_stage<16, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
   }
 }
 
@@ -78,25 +106,34 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, int n, int p, flo
 // barrier.
 template <int DIR, typename C>
 __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, const C* __restrict__ tw) {
+  using Re = typename RealOf<C>::type;
   for (int st = 0; st < s.nst; ++st) {
-    const int p = s.p[st];
-    const float pi = s.pinv[st];
-    switch (s.radix[st]) {
-      case 2: gen_stage<2, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 3: gen_stage<3, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 4: gen_stage<4, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 5: gen_stage<5, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 7: gen_stage<7, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 8: gen_stage<8, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      case 9: gen_stage<9, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-      default: gen_stage<16, DIR>(a, b, s.n, p, pi, s.T, t, tw); break;
-    }
+    gen_stage_any<DIR>(s.radix[st], a, b, static_cast<const C*>(nullptr), static_cast<C*>(nullptr), Re(1), s.n,
+                       s.p[st], s.pinv[st], s.T, t, tw);
     __syncthreads();
     C* tmp = a;
     a = b;
     b = tmp;
   }
   return a;
+}
+
+// All stages from the transform's global input `gin` to its global output
+// `gout` (scaled by `scale` for the inverse): the first stage loads its
+// butterflies straight from HBM and the last stores them there, so only
+// the stages between touch the shared buffers a and b.
+template <int DIR, typename C>
+__device__ __forceinline__ void gen_fft_io(C* a, C* b, const C* gin, C* gout, typename RealOf<C>::type scale,
+                                           const GenSched& s, int t, const C* __restrict__ tw) {
+  for (int st = 0; st < s.nst; ++st) {
+    const bool first = st == 0, last = st + 1 == s.nst;
+    gen_stage_any<DIR>(s.radix[st], a, b, first ? gin : nullptr, last ? gout : nullptr, scale, s.n, s.p[st],
+                       s.pinv[st], s.T, t, tw);
+    if (!last) __syncthreads();
+    C* tmp = a;
+    a = b;
+    b = tmp;
+  }
 }
 
 // Batched C2C with a runtime schedule: B transforms per CTA, T threads each.
@@ -121,22 +158,11 @@ __global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t 
     }
   }
   const int slot = threadIdx.x / s.T, t = threadIdx.x % s.T;
-  C* x = reinterpret_cast<C*>(smem_raw) + slot * s.stride;
   const int64_t b = int64_t(blockIdx.x) * s.B + slot;
   const bool valid = slot < s.B && b < count;
-  const C* in = src + (valid ? b * idist : 0);
-  if (slot < s.B)
-    for (int e = t; e < s.n; e += s.T) x[gpad(e)] = valid ? ld_stream(in + e) : C{0, 0};
-  __syncthreads();
-  const C* res = gen_fft<DIR>(x, x + s.half, s, slot < s.B ? t : kIdleThread, tw);
-  if (valid) {
-    C* out = dst + b * odist;
-    for (int e = t; e < s.n; e += s.T) {
-      C y = res[gpad(e)];
-      if constexpr (DIR > 0) y = cscale(y, scale);
-      st_stream(out + e, y);
-    }
-  }
+  C* x = reinterpret_cast<C*>(smem_raw) + (valid ? slot : 0) * s.stride;
+  gen_fft_io<DIR>(x, x + s.half, src + (valid ? b * idist : 0), dst + (valid ? b * odist : 0), scale, s,
+                  valid ? t : kIdleThread, tw);
 }
 
 }  // namespace gfft
