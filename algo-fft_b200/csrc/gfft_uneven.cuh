@@ -62,14 +62,11 @@ __global__ void __launch_bounds__(1024) k_uneven(const C* src, C* dst, const Une
     const C* in = src + it.off;
     C* out = dst + it.off;
     if (!d.bluestein) {
-      for (int e = tid; e < L; e += nthr) x[gpad(e)] = ld_stream(in + e);
-      __syncthreads();
-      const C* res = gen_fft<DIR>(x, x + d.s.half, d.s, t, W);
-      const Re sc = Re(1.0 / double(L));
-      for (int e = tid; e < L; e += nthr) {
-        C y = res[gpad(e)];
-        if constexpr (DIR > 0) y = cscale(y, sc);
-        st_stream(out + e, y);
+      if (d.s.nst == 0) {  // length 1
+        for (int e = tid; e < L; e += nthr) st_stream(out + e, ld_stream(in + e));
+      } else {
+        // first stage from HBM, last stage to HBM
+        gen_fft_io<DIR>(x, x + d.s.half, in, out, Re(1.0 / double(L)), d.s, t, W);
       }
     } else {
       const int n = int(d.n);
