@@ -86,6 +86,14 @@ cudaError_t exec_pow2_cols(int prec, int dir, void* dst, const void* src, int64_
 // Bluestein as one fused kernel when the FFT length M fits one CTA (M a
 // power of two <= 16384 complex64, <= 8192 complex128).
 bool bluestein_fused_supported(int prec, int64_t M);
+// Bluestein through the two-pass FFT_M with the chain fused into its passes
+// (M = 2^15..2^20, split N1 x M / N1 as the two-pass plans).
+bool bluestein_tp_supported(int prec, int64_t M, int n1);
+size_t bluestein_tp_chunk_bytes(int prec, int64_t M, int64_t count);
+cudaError_t exec_bluestein_tp(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
+                              int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw1,
+                              const void* tw2, BigTwiddle bt, double scale, void* scratch, void* work,
+                              cudaStream_t st);
 cudaError_t exec_bluestein_fused(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
                                  int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw,
                                  double scale, cudaStream_t st);

@@ -386,6 +386,22 @@ static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const v
     if (fe != cudaSuccess) return cuda_status(fe, "k_bs_fused");
     return GFFT_OK;
   }
+  // two-pass FFT_M: the chain fused into its four passes
+  if (c->sub->algo == Algo::TwoPass && bluestein_tp_supported(c->prec, M, c->sub->tp[0]->n1)) {
+    const size_t bytes = bluestein_tp_chunk_bytes(c->prec, M, count);
+    void* buf = nullptr;
+    GFFT_CUDA(ws_alloc(&buf, 2 * bytes, st));
+    BigTwiddle bt;
+    bt.lo = c->sub->bt_lo;
+    bt.hi = c->sub->bt_hi;
+    bt.shift = c->sub->bt_shift;
+    const cudaError_t te = exec_bluestein_tp(c->prec, M, src, dst, count, idist, odist, n, c->bs_w[d], c->bs_f[d],
+                                             c->sub->tw1, c->sub->tw2, bt, dir < 0 ? 1.0 : 1.0 / double(n), buf,
+                                             static_cast<char*>(buf) + bytes, st);
+    cudaFreeAsync(buf, st);
+    if (te != cudaSuccess) return cuda_status(te, "k_bs_tp");
+    return GFFT_OK;
+  }
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
   void* work = nullptr;
   GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&work), size_t(chunk) * size_t(M) * es, st));

@@ -56,14 +56,20 @@ struct ColShape {
 };
 
 // LOAD_SMEM: the tile is already in shared memory (a TMA copy put it there).
-enum { LOAD_STREAM = 0, LOAD_L2 = 1, LOAD_SMEM = 2 };
+// LOAD_FN: the first stage asks the caller's IO object, io.load(row, c).
+enum { LOAD_STREAM = 0, LOAD_L2 = 1, LOAD_SMEM = 2, LOAD_FN = 3 };
 // OUT_SMEM: the result, scaled, back into the tile's rows (for a TMA store);
 // OUT_SMEM_TWIDDLE_T: times the big twiddle, transposed into rows of L + 1
 // elements per column, for a coalesced store of whole columns.
 // OUT_SMEM_TWIDDLE_SW: times the big twiddle, transposed into boxes of 128-byte
 // rows in the copy engine's 128-byte swizzle (see swz128), for TMA stores of
 // whole columns.
-enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1, OUT_SMEM = 2, OUT_SMEM_TWIDDLE_T = 3, OUT_SMEM_TWIDDLE_SW = 4 };
+// OUT_FN: the last stage hands each (row, column, value) to io.store, the
+// value already scaled for the inverse.
+enum { OUT_COLUMNS = 0, OUT_SMEM_TWIDDLE = 1, OUT_SMEM = 2, OUT_SMEM_TWIDDLE_T = 3, OUT_SMEM_TWIDDLE_SW = 4, OUT_FN = 5 };
+
+// Default IO of col_stage: no hooks.
+struct NoIO {};
 
 // Element (row, c) of a transposed tile held as L / RE boxes of NC rows (one
 // per column c) of 128 bytes (RE elements of consecutive rows), in the
@@ -89,11 +95,11 @@ __device__ __forceinline__ C gload(const C* p) {
 // column c is at in[r*ISTRIDE + c].
 // ISTRIDE / OSTRIDE = 0 take the row pitch from `pitch` at run time.
 template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE,
-          bool DENSE = false>
+          bool DENSE = false, typename IO = NoIO>
 __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
                                           int t, int c, bool active, const C* __restrict__ tw,
                                           typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2,
-                                          int64_t pitch = 0) {
+                                          int64_t pitch = 0, const IO& io = IO()) {
   const int64_t IS = ISTRIDE > 0 ? ISTRIDE : pitch;
   const int64_t OS = OSTRIDE > 0 ? OSTRIDE : pitch;
   using S = ColShape<L, EPT, NC, sizeof(C), DENSE>;
@@ -124,7 +130,12 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
   }
 
   if (active) {
-    if constexpr (FIRST && LOADK != LOAD_SMEM) {
+    if constexpr (FIRST && LOADK == LOAD_FN) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < RS; ++r) v[q * RS + r] = io.load(t + q * T + r * STRIDE, c);
+    } else if constexpr (FIRST && LOADK != LOAD_SMEM) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
@@ -148,7 +159,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
     }
   }
 
-  if constexpr (LAST && MODE == OUT_COLUMNS) {
+  if constexpr (LAST && (MODE == OUT_COLUMNS || MODE == OUT_FN)) {
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
@@ -156,7 +167,8 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
         for (int r = 0; r < RS; ++r) {
           C o = v[q * RS + r];
           if constexpr (DIR > 0) o = cscale(o, scale);
-          st_stream(out + int64_t(t + q * T + r * P) * OS + c, o);
+          if constexpr (MODE == OUT_FN) io.store(t + q * T + r * P, c, o);
+          else st_stream(out + int64_t(t + q * T + r * P) * OS + c, o);
         }
     }
   } else if constexpr (LAST && MODE == OUT_SMEM) {
@@ -207,8 +219,8 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
       }
     }
     __syncthreads();
-    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE, DENSE>(v, in, out, sh, t, c, active, tw,
-                                                                                scale, bt, n2, pitch);
+    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE, DENSE, IO>(v, in, out, sh, t, c, active, tw,
+                                                                                    scale, bt, n2, pitch, io);
   }
 }
 

@@ -37,7 +37,7 @@ def _judge(x, n, inverse=False):
 # runtime two-pass range (> one CTA).
 SMOOTH = [3, 5, 6, 7, 9, 12, 15, 21, 49, 60, 100, 243, 343, 360, 1000, 2187, 3125, 6000, 6720, 15625,
           2 * 3 * 5 * 7 * 64, 48000, 50421, 62500, 65536 + 0 * 1]
-PRIMES = [2, 11, 13, 17, 31, 97, 251, 1009, 4099, 8191, 16411, 65521]
+PRIMES = [2, 11, 13, 17, 31, 97, 251, 1009, 4099, 8191, 16411, 65521, 131071, 262147]
 
 
 @pytest.mark.parametrize("n", SMOOTH)
@@ -75,7 +75,7 @@ def test_bluestein_c64(n):
     assert rel_l2(back, x) <= 2 * tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n", [7, 31, 1021, 65521])
+@pytest.mark.parametrize("n", [7, 31, 1021, 16411, 65521, 131071])
 def test_bluestein_c128(n):
     # exact k^2 mod 2n chirps keep complex128 Bluestein at 1e-13*log2N even
     # where the reference's float64(k*k) chirp (bluestein.go:23-29) cannot
