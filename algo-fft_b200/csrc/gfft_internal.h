@@ -94,6 +94,13 @@ cudaError_t exec_bluestein_tp(int prec, int64_t M, const void* src, void* dst, i
                               int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw1,
                               const void* tw2, BigTwiddle bt, double scale, void* scratch, void* work,
                               cudaStream_t st);
+// The same chain over the rows of an uneven batch's Bluestein group: row r
+// is items[r] (offset, length, chirp and filter offsets into tab), the
+// forward tables serving both directions.
+struct BigItem;
+cudaError_t exec_bluestein_tp_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
+                                    int64_t rows, const void* tab, const void* tw1, const void* tw2, BigTwiddle bt,
+                                    void* scratch, void* work, cudaStream_t st);
 cudaError_t exec_bluestein_fused(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
                                  int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw,
                                  double scale, cudaStream_t st);

@@ -16,38 +16,53 @@
 #include <utility>
 #include <vector>
 #include "gfft_internal.h"
+#include "gfft_uneven.cuh"
 #include "kernels_twopass.cuh"
 
 namespace gfft {
 namespace {
 
+// The direction UDIR of the transform the chain serves: the forward chirp
+// w and filter spectrum F serve both directions, the inverse taking conj(w)
+// and conj(F[(M - k) mod M]).  Plans keep tables per direction and run
+// their chain as UDIR = -1 with the tables of the direction asked for.
+template <int UDIR, typename C>
+__device__ __forceinline__ C chirp_of(const C* w, int64_t m) {
+  const C v = __ldg(w + m);
+  if constexpr (UDIR > 0) return cconj(v);
+  else return v;
+}
+
 // chirp-weighted, zero-padded input: m = row * N2 + col0 + c
-template <typename C>
+template <typename C, int UDIR>
 struct BsChirpIn {
   const C* x;  // this transform's input
   const C* w;
   int64_t n, n2, col0;
   __device__ __forceinline__ C load(int row, int c) const {
     const int64_t m = int64_t(row) * n2 + col0 + c;
-    return m < n ? cmul(ld_stream(x + m), __ldg(w + m)) : C{0, 0};
+    return m < n ? cmul(ld_stream(x + m), chirp_of<UDIR>(w, m)) : C{0, 0};
   }
 };
 
 // spectrum times the filter, k = col0 + c + N1 * row, kept in L2 for the
 // inverse FFT that reads it next
-template <typename C>
+template <typename C, int UDIR>
 struct BsFilterOut {
   C* y;  // this transform's work row
   const C* f;
-  int64_t n1, col0;
+  int64_t n1, col0, m;
   __device__ __forceinline__ void store(int row, int c, C v) const {
     const int64_t k = col0 + c + n1 * int64_t(row);
-    __stcg(y + k, cmul(v, __ldg(f + k)));
+    C fk;
+    if constexpr (UDIR > 0) fk = cconj(__ldg(f + ((m - k) & (m - 1))));
+    else fk = __ldg(f + k);
+    __stcg(y + k, cmul(v, fk));
   }
 };
 
-// outputs k < n times the chirp and the user scale (1/M is already in v)
-template <typename C>
+// outputs k < n times the chirp and the row's scale (1/M is already in v)
+template <typename C, int UDIR>
 struct BsChirpOut {
   C* y;  // this transform's output
   const C* w;
@@ -55,27 +70,52 @@ struct BsChirpOut {
   typename RealOf<C>::type scale;
   __device__ __forceinline__ void store(int row, int c, C v) const {
     const int64_t k = col0 + c + n1 * int64_t(row);
-    if (k < n) st_stream(y + k, cscale(cmul(v, __ldg(w + k)), scale));
+    if (k < n) st_stream(y + k, cscale(cmul(v, chirp_of<UDIR>(w, k)), scale));
   }
 };
 
 struct BsTpParams {
-  const void* x;     // user input
-  void* out;         // user output
+  const void* x;     // user input (items: the packed batch)
+  void* out;         // user output (items: the packed batch)
   void* scratch;     // pass-1 intermediate, chunk x M
   void* work;        // spectrum times filter, chunk x M
-  const void* w;     // chirp of the direction
-  const void* f;     // filter spectrum of the direction
+  const void* w;     // chirp (plans)
+  const void* f;     // filter spectrum (plans)
+  const BigItem* items;  // per-transform offsets, lengths and tables, or null
+  const void* tab;       // the tables items point into
   const void* tw1;   // W_N1
   const void* tw2;   // W_N2
   BigTwiddle bt;     // W_M
   int64_t n, idist, odist;
-  double inv_m, scale;
+  double inv_m, scale;  // items: the scale is 1/n for the inverse, else 1
 };
+
+// One transform's buffers and parameters.
+template <typename C>
+struct BsRow {
+  const C* x;
+  C* y;
+  const C* w;
+  const C* f;
+  int64_t n;
+  double scale;
+};
+
+template <typename C, int UDIR>
+__device__ __forceinline__ BsRow<C> bs_row(const BsTpParams& p, int64_t b) {
+  if (p.items) {
+    const BigItem it = p.items[b];
+    const C* tab = static_cast<const C*>(p.tab);
+    return BsRow<C>{static_cast<const C*>(p.x) + it.off, static_cast<C*>(p.out) + it.off, tab + it.chirp,
+                    tab + it.filt, it.n, UDIR > 0 ? 1.0 / double(it.n) : 1.0};
+  }
+  return BsRow<C>{static_cast<const C*>(p.x) + b * p.idist, static_cast<C*>(p.out) + b * p.odist,
+                  static_cast<const C*>(p.w), static_cast<const C*>(p.f), p.n, p.scale};
+}
 
 enum { BS_FWD1 = 0, BS_FWD2 = 1, BS_INV2 = 2 };
 
-template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int KIND>
+template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int KIND, int UDIR>
 __global__ void __launch_bounds__(TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, -1>::TPB,
                                   TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, -1>::MIN_BLOCKS)
 k_bs_tp(BsTpParams p, int64_t b0) {
@@ -93,10 +133,10 @@ k_bs_tp(BsTpParams p, int64_t b0) {
     const int col0 = int(blockIdx.x % TP::TILES1) * NC1;
     const bool active = tid < S1::TPB;
     const int c = tid % NC1, t = tid / NC1;
-    const BsChirpIn<C> io{static_cast<const C*>(p.x) + (b0 + bl) * p.idist, static_cast<const C*>(p.w), p.n, N2,
-                          col0};
+    const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
+    const BsChirpIn<C, UDIR> io{rw.x, rw.w, rw.n, N2, col0};
     C* y = scratch + bl * TP::N;
-    col_stage<C, N1, EPT1, NC1, -1, 1, LOAD_FN, OUT_SMEM_TWIDDLE, N2, 0, false, BsChirpIn<C>>(
+    col_stage<C, N1, EPT1, NC1, -1, 1, LOAD_FN, OUT_SMEM_TWIDDLE, N2, 0, false, BsChirpIn<C, UDIR>>(
         v, nullptr, nullptr, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c), 0,
         io);
     for (int e = tid; e < N1 * NC1; e += TP::TPB) {
@@ -109,14 +149,14 @@ k_bs_tp(BsTpParams p, int64_t b0) {
     const bool active = tid < S2::TPB;
     const int c = tid % NC2, t = tid / NC2;
     const C* y = scratch + bl * TP::N + col0;
+    const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
     if constexpr (KIND == BS_FWD2) {
-      const BsFilterOut<C> io{static_cast<C*>(p.work) + bl * TP::N, static_cast<const C*>(p.f), N1, col0};
-      col_stage<C, N2, EPT2, NC2, -1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsFilterOut<C>>(
+      const BsFilterOut<C, UDIR> io{static_cast<C*>(p.work) + bl * TP::N, rw.f, N1, col0, TP::N};
+      col_stage<C, N2, EPT2, NC2, -1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsFilterOut<C, UDIR>>(
           v, y, nullptr, sh, t, c, active, static_cast<const C*>(p.tw2), Re(1), p.bt, 0, 0, io);
     } else {
-      const BsChirpOut<C> io{static_cast<C*>(p.out) + (b0 + bl) * p.odist, static_cast<const C*>(p.w), p.n, N1, col0,
-                             Re(p.scale)};
-      col_stage<C, N2, EPT2, NC2, +1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsChirpOut<C>>(
+      const BsChirpOut<C, UDIR> io{rw.y, rw.w, rw.n, N1, col0, Re(rw.scale)};
+      col_stage<C, N2, EPT2, NC2, +1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsChirpOut<C, UDIR>>(
           v, y, nullptr, sh, t, c, active, static_cast<const C*>(p.tw2), Re(p.inv_m), p.bt, 0, 0, io);
     }
   }
@@ -127,8 +167,8 @@ struct BsTpKernel {
   int64_t m;
   int n1;
   int tpb, smem;
-  const void* fn[4];  // the three fused passes and this file's plain inverse first pass
-  cudaError_t (*run)(const BsTpParams& p, int64_t count, void* scratch, void* work, cudaStream_t st);
+  const void* fn[7];  // the fused passes (UDIR = -1, then +1) and this file's plain inverse first pass
+  cudaError_t (*run)(const BsTpParams& p, int udir, int64_t count, void* scratch, void* work, cudaStream_t st);
 };
 
 std::vector<BsTpKernel>& table() {
@@ -142,39 +182,43 @@ struct BsTpOf {
   using A = TileRule<TE, EMAX, N1>;
   using B = TileRule<TE, EMAX, N2>;
   using TP = TwoPass<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, -1>;
-  template <int KIND>
+  template <int KIND, int UDIR>
   static const void* fn() {
-    return reinterpret_cast<const void*>(&k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, KIND>);
+    return reinterpret_cast<const void*>(&k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, KIND, UDIR>);
   }
-  // The whole chain over `count` transforms in chunks that fill the
-  // scratch and work buffers (bluestein_tp_chunk_bytes each).
-  static cudaError_t run(const BsTpParams& p0, int64_t count, void* scratch, void* work, cudaStream_t st) {
-    BsTpParams p = p0;
-    p.scratch = scratch;
-    p.work = work;
+  template <int UDIR>
+  static cudaError_t run_dir(const BsTpParams& p, int64_t count, cudaStream_t st) {
     const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (TP::N * int64_t(sizeof(C)))));
     TwoPassParams q{};
-    q.scratch = scratch;
+    q.scratch = p.scratch;
+    q.src = p.work;
     q.idist = TP::N;
     q.tw1 = p.tw1;
     q.tw2 = p.tw2;
     q.bt = p.bt;
     for (int64_t b0 = 0; b0 < count; b0 += chunk) {
       const int64_t nb = std::min(chunk, count - b0);
-      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD1>
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD1, UDIR>
           <<<unsigned(nb * TP::TILES1), TP::TPB, TP::SMEM, st>>>(p, b0);
-      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD2>
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD2, UDIR>
           <<<unsigned(nb * TP::TILES2), TP::TPB, TP::SMEM, st>>>(p, b0);
       // inverse FFT, first pass: plain, from the work rows into scratch
-      q.src = work;
       k_tp_split<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, +1, 1>
           <<<unsigned(nb * TP::TILES1), TP::TPB, TP::SMEM, st>>>(q, 0);
-      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_INV2>
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_INV2, UDIR>
           <<<unsigned(nb * TP::TILES2), TP::TPB, TP::SMEM, st>>>(p, b0);
       const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+  }
+  // The whole chain over `count` transforms in chunks that fill the
+  // scratch and work buffers (bluestein_tp_chunk_bytes each).
+  static cudaError_t run(const BsTpParams& p0, int udir, int64_t count, void* scratch, void* work, cudaStream_t st) {
+    BsTpParams p = p0;
+    p.scratch = scratch;
+    p.work = work;
+    return udir < 0 ? run_dir<-1>(p, count, st) : run_dir<+1>(p, count, st);
   }
 };
 
@@ -187,10 +231,13 @@ void reg() {
   k.n1 = N1;
   k.tpb = O::TP::TPB;
   k.smem = O::TP::SMEM;
-  k.fn[0] = O::template fn<BS_FWD1>();
-  k.fn[1] = O::template fn<BS_FWD2>();
-  k.fn[2] = O::template fn<BS_INV2>();
-  k.fn[3] = reinterpret_cast<const void*>(
+  k.fn[0] = O::template fn<BS_FWD1, -1>();
+  k.fn[1] = O::template fn<BS_FWD2, -1>();
+  k.fn[2] = O::template fn<BS_INV2, -1>();
+  k.fn[3] = O::template fn<BS_FWD1, +1>();
+  k.fn[4] = O::template fn<BS_FWD2, +1>();
+  k.fn[5] = O::template fn<BS_INV2, +1>();
+  k.fn[6] = reinterpret_cast<const void*>(
       &k_tp_split<C, N1, O::A::EPT, O::A::NC, N2, O::B::EPT, O::B::NC, +1, 1>);
   k.run = &O::run;
   table().push_back(k);
@@ -227,44 +274,73 @@ size_t bluestein_tp_chunk_bytes(int prec, int64_t M, int64_t count) {
   return size_t(chunk) * size_t(M) * size_t(es);
 }
 
+namespace {
+
+const BsTpKernel* bs_tp_ready(int prec, int64_t M, cudaError_t* err) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> done;  // (kernel, device) with the smem limit raised
+  *err = cudaSuccess;
+  for (const auto& k : table()) {
+    if (k.prec != prec || k.m != M) continue;
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (std::find(done.begin(), done.end(), std::make_pair(k.fn[0], dev)) == done.end()) {
+      if (k.smem > 48 * 1024)
+        for (const void* f : k.fn) {
+          *err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+          if (*err != cudaSuccess) return nullptr;
+        }
+      done.push_back({k.fn[0], dev});
+    }
+    return &k;
+  }
+  *err = cudaErrorNotSupported;
+  return nullptr;
+}
+
+}  // namespace
+
 cudaError_t exec_bluestein_tp(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
                               int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw1,
                               const void* tw2, BigTwiddle bt, double scale, void* scratch, void* work,
                               cudaStream_t st) {
-  static std::mutex mu;
-  static std::vector<std::pair<const void*, int>> done;  // (kernel, device) with the smem limit raised
-  for (const auto& k : table()) {
-    if (k.prec != prec || k.m != M) continue;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    {
-      std::lock_guard<std::mutex> g(mu);
-      if (std::find(done.begin(), done.end(), std::make_pair(k.fn[0], dev)) == done.end()) {
-        if (k.smem > 48 * 1024)
-          for (const void* f : k.fn) {
-            e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
-            if (e != cudaSuccess) return e;
-          }
-        done.push_back({k.fn[0], dev});
-      }
-    }
-    BsTpParams p{};
-    p.x = src;
-    p.out = dst;
-    p.w = chirp;
-    p.f = filt;
-    p.tw1 = tw1;
-    p.tw2 = tw2;
-    p.bt = bt;
-    p.n = n;
-    p.idist = idist;
-    p.odist = odist;
-    p.inv_m = 1.0 / double(M);
-    p.scale = scale;
-    return k.run(p, count, scratch, work, st);
-  }
-  return cudaErrorNotSupported;
+  cudaError_t e;
+  const BsTpKernel* k = bs_tp_ready(prec, M, &e);
+  if (!k) return e;
+  BsTpParams p{};
+  p.x = src;
+  p.out = dst;
+  p.w = chirp;
+  p.f = filt;
+  p.tw1 = tw1;
+  p.tw2 = tw2;
+  p.bt = bt;
+  p.n = n;
+  p.idist = idist;
+  p.odist = odist;
+  p.inv_m = 1.0 / double(M);
+  p.scale = scale;
+  return k->run(p, -1, count, scratch, work, st);
+}
+
+cudaError_t exec_bluestein_tp_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
+                                    int64_t rows, const void* tab, const void* tw1, const void* tw2, BigTwiddle bt,
+                                    void* scratch, void* work, cudaStream_t st) {
+  cudaError_t e;
+  const BsTpKernel* k = bs_tp_ready(prec, M, &e);
+  if (!k) return e;
+  BsTpParams p{};
+  p.x = src;
+  p.out = dst;
+  p.items = items;
+  p.tab = tab;
+  p.tw1 = tw1;
+  p.tw2 = tw2;
+  p.bt = bt;
+  p.inv_m = 1.0 / double(M);
+  return k->run(p, dir, rows, scratch, work, st);
 }
 
 }  // namespace gfft
