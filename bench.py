@@ -229,19 +229,42 @@ def _median_ms(fn, stream, iters: int, warm: int = 1) -> float:
     return statistics.median(ts)
 
 
-def extras(dev, stream, iters: int) -> dict:
+EXTRAS = ("c128_sweep", "real", "uneven", "mixed_radix", "bluestein", "precision_form", "convolve")
+
+
+def extras(dev, stream, iters: int, only=EXTRAS) -> dict:
     """Device-timed figures of the other measured workloads (median of
-    `iters` runs after one warm-up), each with its own accuracy check."""
-    import numpy as np
+    `iters` runs after one warm-up), each with its own accuracy check;
+    `only` names the ones to run."""
     import torch
-    import algofft
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
     out = {}
     gen = torch.Generator(device=dev)
     gen.manual_seed(77)
+    if "c128_sweep" in only:
+        out.update(_c128_sweep(dev, stream, iters, gen))
+    if "real" in only:
+        out.update(_real(dev, stream, iters, gen))
+    if "uneven" in only:
+        out.update(_uneven(dev, stream, iters, gen))
+    if "mixed_radix" in only:
+        out.update(_mixed_radix(dev, stream, iters, gen))
+    if "bluestein" in only:
+        out.update(_bluestein(dev, stream, iters, gen))
+    if "precision_form" in only:
+        out.update(_precision_form(dev, stream, iters, gen))
+    if "convolve" in only:
+        out.update(_convolve(dev, stream, iters, gen))
+    return out
 
-    # complex128 sweep, 1 GiB batches
+
+def _c128_sweep(dev, stream, iters, gen):
+    """Complex128 power-of-two sweep, 1 GiB batches."""
+    import numpy as np
+    import torch
+    import algofft
+    import oracle
+    out = {}
     x = torch.randn(BUF_BYTES // 8, generator=gen, device=dev, dtype=torch.float64).view(torch.complex128)
     y = torch.empty_like(x)
     c128 = {}
@@ -257,8 +280,15 @@ def extras(dev, stream, iters: int) -> dict:
     out["c128_sweep"] = {"unit": "GB/s", "bytes_per_transform": "32*N", "per_size_gbs": c128,
                          "rel_l2_vs_fp64_n4096": err128}
     del x, y
+    return out
 
-    # R2C / C2R float32, N = 4096, batch 65536
+
+def _real(dev, stream, iters, gen):
+    """R2C / C2R float32, N = 4096, batch 65536."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
     n, batch = 4096, 65536
     xr = torch.rand(n * batch, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
     X = torch.empty(batch * (n // 2 + 1), dtype=torch.complex64, device=dev)
@@ -273,8 +303,15 @@ def extras(dev, stream, iters: int) -> dict:
                               "r2c_gbs": rb * batch / (f_ms / 1e3) / 1e9, "c2r_gbs": rb * batch / (i_ms / 1e3) / 1e9,
                               "rel_l2_vs_fp64": err}
     del xr, X, back
+    return out
 
-    # uneven-length batch: one plan, graph replay, against the per-size path
+
+def _uneven(dev, stream, iters, gen):
+    """Uneven-length batch: one plan, graph replay, against the per-size path."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
     L = algofft.uneven_lengths(20000, seed=0)
     with algofft.PlanUneven(L) as p:
         tot = p.Total()
@@ -298,9 +335,60 @@ def extras(dev, stream, iters: int) -> dict:
                            "gbs_user_bytes": 16 * tot / (g_ms / 1e3) / 1e9,
                            "max_rel_l2_first_40": max(errs)}
     del xu, yu
+    return out
 
-    # precision form: tensor-core split-fp16 radix-16 stages against the FP32
-    # CUDA-core path, complex64, batches of 2 GiB, two input sets
+
+def _mixed_radix(dev, stream, iters, gen):
+    """7-smooth lengths (runtime radix, one CTA or two passes), complex64,
+    512 MiB batches; GB/s of user bytes and the error of the first
+    transforms against numpy's FP64 FFT."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
+    for n in (60, 1000, 6000, 6561, 10000, 50421, 100000):
+        count = (1 << 29) // (8 * n)
+        x = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+        y = torch.empty_like(x)
+        with algofft.NewPlan(n) as p:
+            ms = _median_ms(lambda: p.ForwardBatch(y, x, count), stream, iters)
+            alg = p.Algorithm()
+        ref = np.fft.fft(x[:2 * n].cpu().numpy().astype(np.complex128).reshape(2, n), axis=1).ravel()
+        err = float(np.linalg.norm(y[:2 * n].cpu().numpy() - ref) / np.linalg.norm(ref))
+        out[str(n)] = {"algorithm": alg, "gbs": 16 * n * count / (ms / 1e3) / 1e9, "rel_l2_vs_fp64": err}
+        del x, y
+    return {"mixed_radix_c64_512MiB": out}
+
+
+def _bluestein(dev, stream, iters, gen):
+    """Prime lengths (Bluestein), complex64, 512 MiB batches; GB/s of user
+    bytes (the two FFTs run over M >= 2n points) and the error."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
+    for n in (1009, 8191, 16411, 65521, 131071):
+        count = max(1, (1 << 29) // (8 * n))
+        x = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+        y = torch.empty_like(x)
+        with algofft.NewPlan(n) as p:
+            ms = _median_ms(lambda: p.ForwardBatch(y, x, count), stream, iters)
+            alg = p.Algorithm()
+        k = min(count, 2)
+        ref = np.fft.fft(x[:k * n].cpu().numpy().astype(np.complex128).reshape(k, n), axis=1).ravel()
+        err = float(np.linalg.norm(y[:k * n].cpu().numpy() - ref) / np.linalg.norm(ref))
+        out[str(n)] = {"algorithm": alg, "gbs_user_bytes": 16 * n * count / (ms / 1e3) / 1e9, "rel_l2_vs_fp64": err}
+        del x, y
+    return {"bluestein_c64_512MiB": out}
+
+
+def _precision_form(dev, stream, iters, gen):
+    """Tensor-core split-fp16 radix-16 stages against the FP32 CUDA-core
+    path, complex64, batches of 2 GiB, two input sets."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
     tcr = {}
     peak_tf = tensor_peak()
     for n in (256, 4096, 65536, 1 << 20):
@@ -340,8 +428,15 @@ def extras(dev, stream, iters: int) -> dict:
     out["precision_form_c64_2GiB"] = {"tolerance": "rel L2 <= 1e-6*log2(N)", "bf16_peak_tflops": peak_tf,
                                       "flops_convention": "GEMM-equivalent: 3 split products x 2*32*32 per "
                                                           "radix-16 butterfly per stage", "per_size": tcr}
+    return out
 
-    # ConvolveReal: 64 signals of 2^20 reals with a 4097-tap kernel
+
+def _convolve(dev, stream, iters, gen):
+    """ConvolveReal: 64 signals of 2^20 reals with a 4097-tap kernel."""
+    import numpy as np
+    import torch
+    import algofft
+    out = {}
     cnt, na, nb = 64, 1 << 20, 4097
     a = torch.rand(cnt * na, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
     k = torch.rand(nb, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
@@ -366,6 +461,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-slice leg (profiling runs)")
     ap.add_argument("--no-extras", action="store_true", help="skip the c128/real/uneven/convolve figures")
+    ap.add_argument("--extras", default=",".join(EXTRAS), help="comma-separated extras to run: " + ",".join(EXTRAS))
     ap.add_argument("--sizes", default="", help="comma-separated subset of lengths (profiling runs)")
     ap.add_argument("--batch-mib", type=int, default=BUF_BYTES >> 20, help="batch bytes per length in MiB")
     args = ap.parse_args()
@@ -498,7 +594,7 @@ def main():
         del xin, yout
         bufs = {n: (None, None, b[2]) for n, b in bufs.items()}
         torch.cuda.empty_cache()
-        ext = extras(dev, stream, max(3, min(args.steps, 10)))
+        ext = extras(dev, stream, max(3, min(args.steps, 10)), tuple(args.extras.split(",")))
 
     if rank == 0:
         line = {
