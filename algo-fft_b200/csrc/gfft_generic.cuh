@@ -199,8 +199,9 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
   const C* in = src + (valid ? b * in_dist : 0);
   C* out = dst + (valid ? b * out_dist : 0);
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const int ncs = __ffs(NC) - 1;  // NC is a power of two
   for (int e = tid; e < L * NC; e += nthr) {
-    const int row = e / NC, c = e % NC;
+    const int row = e >> ncs, c = e & (NC - 1);
     C v = C{0, 0};
     if (valid && col0 + c < ncols) {
       const C* p = in + int64_t(row) * pitch + col0 + c;
@@ -219,18 +220,21 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
     const C* lo = static_cast<const C*>(bt.lo);
     const C* hi = static_cast<const C*>(bt.hi);
     const int64_t mask = (int64_t(1) << bt.shift) - 1;
-    for (int e = tid; e < L * NC; e += nthr) {
-      const int c = e / L, k1 = e % L;
+    // column by column, rows k1 across the threads (runs of L in HBM)
+    for (int c = 0; c < NC; ++c) {
       const int64_t n2 = col0 + c;
-      if (n2 >= ncols) continue;
-      const int64_t m = n2 * k1;
-      C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
-      if constexpr (DIR > 0) w.y = -w.y;
-      __stcg(out + n2 * L + k1, cmul(res[c * s.stride + gpad(k1)], w));
+      if (n2 >= ncols) break;
+      const C* rc = res + c * s.stride;
+      for (int k1 = tid; k1 < L; k1 += nthr) {
+        const int64_t m = n2 * k1;
+        C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
+        if constexpr (DIR > 0) w.y = -w.y;
+        __stcg(out + n2 * L + k1, cmul(rc[gpad(k1)], w));
+      }
     }
   } else {
     for (int e = tid; e < L * NC; e += nthr) {
-      const int k2 = e / NC, c = e % NC;
+      const int k2 = e >> ncs, c = e & (NC - 1);
       if (col0 + c >= ncols) continue;
       C v = res[c * s.stride + gpad(k2)];
       if constexpr (DIR > 0) v = cscale(v, scale);

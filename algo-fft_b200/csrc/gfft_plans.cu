@@ -250,7 +250,7 @@ static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const
                                     int64_t idist, int64_t odist, cudaStream_t st) {
   const size_t es = elem_bytes(c->prec);
   const int64_t n = c->n;
-  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(64) << 20) / (n * int64_t(es))));
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(512) << 20) / (n * int64_t(es))));
   void* scratch = nullptr;
   GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&scratch), size_t(chunk) * size_t(n) * es, st));
   BigTwiddle bt{c->bt_lo, c->bt_hi, c->bt_shift};
