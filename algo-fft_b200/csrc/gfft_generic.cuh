@@ -53,11 +53,11 @@ __device__ __forceinline__ int gen_mod(int i, int p, float pinv, int& q) {
 }
 
 // One stage: butterflies i = t, t + T, ... of radix R from `in` to `out`
-// (shared memory, padded).  When set, `gin` replaces `in` by the
-// transform's global input (first stage) and `gout` replaces `out` by its
-// global output (last stage, scaled for the inverse); consecutive threads
-// touch consecutive elements of both.
-template <int R, int DIR, typename C>
+// (shared memory, padded).  GI: the stage reads the transform's global
+// input `gin` instead of `in` (first stage); GO: it writes the global
+// output `gout` instead of `out`, scaled for the inverse (last stage).
+// Consecutive threads touch consecutive elements of both.
+template <int R, int DIR, bool GI, bool GO, typename C>
 __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* gout, typename RealOf<C>::type scale,
                                           int n, int p, float pinv, int T, int t, const C* __restrict__ tw) {
   const int nb = n / R;
@@ -65,7 +65,10 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* 
   for (int i = t; i < nb; i += T) {
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = gin ? ld_stream(gin + i + r * nb) : in[gpad(i + r * nb)];
+    for (int r = 0; r < R; ++r) {
+      if constexpr (GI) v[r] = ld_stream(gin + i + r * nb);
+      else v[r] = in[gpad(i + r * nb)];
+    }
     int q;
     const int k = gen_mod(i, p, pinv, q);
     if (p > 1) apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
@@ -73,7 +76,7 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* 
     const int j = q * p * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      if (gout) {
+      if constexpr (GO) {
         C o = v[r];
         if constexpr (DIR > 0) o = cscale(o, scale);
         st_stream(gout + j + r * p, o);
@@ -84,19 +87,19 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* 
   }
 }
 
-template <int DIR, typename C>
+template <int DIR, bool GI, bool GO, typename C>
 __device__ __forceinline__ void gen_stage_any(int radix, const C* a, C* b, const C* gin, C* gout,
                                               typename RealOf<C>::type scale, int n, int p, float pi, int T, int t,
                                               const C* __restrict__ tw) {
   switch (radix) {
-    case 2: gen_stage<2, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 3: gen_stage<3, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 4: gen_stage<4, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 5: gen_stage<5, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 7: gen_stage<7, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 8: gen_stage<8, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 9: gen_stage<9, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    default: gen_stage<16, DIR>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 2: gen_stage<2, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 3: gen_stage<3, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 4: gen_stage<4, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 5: gen_stage<5, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 7: gen_stage<7, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 8: gen_stage<8, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 9: gen_stage<9, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    default: gen_stage<16, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
   }
 }
 
@@ -108,8 +111,8 @@ template <int DIR, typename C>
 __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, const C* __restrict__ tw) {
   using Re = typename RealOf<C>::type;
   for (int st = 0; st < s.nst; ++st) {
-    gen_stage_any<DIR>(s.radix[st], a, b, static_cast<const C*>(nullptr), static_cast<C*>(nullptr), Re(1), s.n,
-                       s.p[st], s.pinv[st], s.T, t, tw);
+    gen_stage_any<DIR, false, false>(s.radix[st], a, b, static_cast<const C*>(nullptr), static_cast<C*>(nullptr),
+                                     Re(1), s.n, s.p[st], s.pinv[st], s.T, t, tw);
     __syncthreads();
     C* tmp = a;
     a = b;
@@ -125,15 +128,21 @@ __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, cons
 template <int DIR, typename C>
 __device__ __forceinline__ void gen_fft_io(C* a, C* b, const C* gin, C* gout, typename RealOf<C>::type scale,
                                            const GenSched& s, int t, const C* __restrict__ tw) {
-  for (int st = 0; st < s.nst; ++st) {
-    const bool first = st == 0, last = st + 1 == s.nst;
-    gen_stage_any<DIR>(s.radix[st], a, b, first ? gin : nullptr, last ? gout : nullptr, scale, s.n, s.p[st],
-                       s.pinv[st], s.T, t, tw);
-    if (!last) __syncthreads();
+  if (s.nst == 1) {
+    gen_stage_any<DIR, true, true>(s.radix[0], a, b, gin, gout, scale, s.n, s.p[0], s.pinv[0], s.T, t, tw);
+    return;
+  }
+  gen_stage_any<DIR, true, false>(s.radix[0], a, b, gin, gout, scale, s.n, s.p[0], s.pinv[0], s.T, t, tw);
+  __syncthreads();
+  for (int st = 1; st + 1 < s.nst; ++st) {
     C* tmp = a;
     a = b;
     b = tmp;
+    gen_stage_any<DIR, false, false>(s.radix[st], a, b, gin, gout, scale, s.n, s.p[st], s.pinv[st], s.T, t, tw);
+    __syncthreads();
   }
+  const int last = s.nst - 1;
+  gen_stage_any<DIR, false, true>(s.radix[last], b, a, gin, gout, scale, s.n, s.p[last], s.pinv[last], s.T, t, tw);
 }
 
 // Batched C2C with a runtime schedule: B transforms per CTA, T threads each.
