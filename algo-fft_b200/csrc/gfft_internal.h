@@ -101,6 +101,11 @@ struct BigItem;
 cudaError_t exec_bluestein_tp_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
                                     int64_t rows, const void* tab, const void* tw1, const void* tw2, BigTwiddle bt,
                                     void* scratch, void* work, cudaStream_t st);
+// Plain FFTs of length M (two-pass, the same split) of an uneven batch's
+// rows, read and written in place in the packed batch.
+cudaError_t exec_twopass_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
+                               int64_t rows, const void* tw1, const void* tw2, BigTwiddle bt, void* scratch,
+                               cudaStream_t st);
 cudaError_t exec_bluestein_fused(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
                                  int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw,
                                  double scale, cudaStream_t st);

@@ -283,6 +283,21 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
     if (rows == 0) continue;
     C* work = static_cast<C*>(g.work);
     const C* tab = static_cast<const C*>(p->tab);
+    if (!g.bluestein && g.plan->algo == Algo::TwoPass && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
+      // one large length on the two-pass FFT: rows read and written in
+      // place in the packed batch, no gather or scatter pass
+      void* scratch = nullptr;
+      GFFT_CUDA(ws_alloc(&scratch, bluestein_tp_chunk_bytes(p->prec, g.M, rows), st));
+      BigTwiddle bt;
+      bt.lo = g.plan->bt_lo;
+      bt.hi = g.plan->bt_hi;
+      bt.shift = g.plan->bt_shift;
+      const cudaError_t e = exec_twopass_items(p->prec, g.M, DIR, src, dst, g.d_items, rows, g.plan->tw1,
+                                               g.plan->tw2, bt, scratch, st);
+      cudaFreeAsync(scratch, st);
+      GFFT_CUDA(e);
+      continue;
+    }
     if (g.bluestein && g.plan->algo == Algo::TwoPass && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
       // the chain fused into the two-pass FFT_M: rows read and written in
       // place in the packed batch, no gather or scatter pass

@@ -113,7 +113,23 @@ __device__ __forceinline__ BsRow<C> bs_row(const BsTpParams& p, int64_t b) {
                   static_cast<const C*>(p.w), static_cast<const C*>(p.f), p.n, p.scale};
 }
 
-enum { BS_FWD1 = 0, BS_FWD2 = 1, BS_INV2 = 2 };
+// Plain transform of an item of length M: reads and writes it in place in
+// the packed batch (uneven groups of one large length).
+template <typename C>
+struct ItemIn {
+  const C* x;
+  int64_t n2, col0;
+  __device__ __forceinline__ C load(int row, int c) const { return ld_stream(x + int64_t(row) * n2 + col0 + c); }
+};
+
+template <typename C>
+struct ItemOut {
+  C* y;
+  int64_t n1, col0;
+  __device__ __forceinline__ void store(int row, int c, C v) const { st_stream(y + col0 + c + n1 * int64_t(row), v); }
+};
+
+enum { BS_FWD1 = 0, BS_FWD2 = 1, BS_INV2 = 2, PL_1 = 3, PL_2 = 4 };
 
 template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int KIND, int UDIR>
 __global__ void __launch_bounds__(TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, -1>::TPB,
@@ -128,7 +144,31 @@ k_bs_tp(BsTpParams p, int64_t b0) {
   const int tid = threadIdx.x;
   C* scratch = static_cast<C*>(p.scratch);
   C v[TP::EPT];
-  if constexpr (KIND == BS_FWD1) {
+  if constexpr (KIND == PL_1) {
+    const int64_t bl = blockIdx.x / TP::TILES1;
+    const int col0 = int(blockIdx.x % TP::TILES1) * NC1;
+    const bool active = tid < S1::TPB;
+    const int c = tid % NC1, t = tid / NC1;
+    const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
+    const ItemIn<C> io{rw.x, N2, col0};
+    C* y = scratch + bl * TP::N;
+    col_stage<C, N1, EPT1, NC1, UDIR, 1, LOAD_FN, OUT_SMEM_TWIDDLE, N2, 0, false, ItemIn<C>>(
+        v, nullptr, nullptr, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c), 0, io);
+    for (int e = tid; e < N1 * NC1; e += TP::TPB) {
+      const int cc = e / N1, row = e % N1;
+      __stcg(y + int64_t(col0 + cc) * N1 + row, sh[S1::phys(row, cc)]);
+    }
+  } else if constexpr (KIND == PL_2) {
+    const int64_t bl = blockIdx.x / TP::TILES2;
+    const int col0 = int(blockIdx.x % TP::TILES2) * NC2;
+    const bool active = tid < S2::TPB;
+    const int c = tid % NC2, t = tid / NC2;
+    const C* y = scratch + bl * TP::N + col0;
+    const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
+    const ItemOut<C> io{rw.y, N1, col0};
+    col_stage<C, N2, EPT2, NC2, UDIR, 1, LOAD_L2, OUT_FN, N1, N1, false, ItemOut<C>>(
+        v, y, nullptr, sh, t, c, active, static_cast<const C*>(p.tw2), Re(p.inv_m), p.bt, 0, 0, io);
+  } else if constexpr (KIND == BS_FWD1) {
     const int64_t bl = blockIdx.x / TP::TILES1;
     const int col0 = int(blockIdx.x % TP::TILES1) * NC1;
     const bool active = tid < S1::TPB;
@@ -167,8 +207,9 @@ struct BsTpKernel {
   int64_t m;
   int n1;
   int tpb, smem;
-  const void* fn[7];  // the fused passes (UDIR = -1, then +1) and this file's plain inverse first pass
+  const void* fn[11];  // fused Bluestein passes (UDIR -1, +1), this file's plain inverse first pass, item passes
   cudaError_t (*run)(const BsTpParams& p, int udir, int64_t count, void* scratch, void* work, cudaStream_t st);
+  cudaError_t (*run_plain)(const BsTpParams& p, int udir, int64_t count, void* scratch, cudaStream_t st);
 };
 
 std::vector<BsTpKernel>& table() {
@@ -212,6 +253,27 @@ struct BsTpOf {
     }
     return cudaSuccess;
   }
+  template <int UDIR>
+  static cudaError_t plain_dir(const BsTpParams& p, int64_t count, cudaStream_t st) {
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (TP::N * int64_t(sizeof(C)))));
+    for (int64_t b0 = 0; b0 < count; b0 += chunk) {
+      const int64_t nb = std::min(chunk, count - b0);
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, PL_1, UDIR>
+          <<<unsigned(nb * TP::TILES1), TP::TPB, TP::SMEM, st>>>(p, b0);
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, PL_2, UDIR>
+          <<<unsigned(nb * TP::TILES2), TP::TPB, TP::SMEM, st>>>(p, b0);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  // Plain FFTs of items (length M) in place in the packed batch, chunks of
+  // bluestein_tp_chunk_bytes of scratch.
+  static cudaError_t run_plain(const BsTpParams& p0, int udir, int64_t count, void* scratch, cudaStream_t st) {
+    BsTpParams p = p0;
+    p.scratch = scratch;
+    return udir < 0 ? plain_dir<-1>(p, count, st) : plain_dir<+1>(p, count, st);
+  }
   // The whole chain over `count` transforms in chunks that fill the
   // scratch and work buffers (bluestein_tp_chunk_bytes each).
   static cudaError_t run(const BsTpParams& p0, int udir, int64_t count, void* scratch, void* work, cudaStream_t st) {
@@ -239,7 +301,12 @@ void reg() {
   k.fn[5] = O::template fn<BS_INV2, +1>();
   k.fn[6] = reinterpret_cast<const void*>(
       &k_tp_split<C, N1, O::A::EPT, O::A::NC, N2, O::B::EPT, O::B::NC, +1, 1>);
+  k.fn[7] = O::template fn<PL_1, -1>();
+  k.fn[8] = O::template fn<PL_2, -1>();
+  k.fn[9] = O::template fn<PL_1, +1>();
+  k.fn[10] = O::template fn<PL_2, +1>();
   k.run = &O::run;
+  k.run_plain = &O::run_plain;
   table().push_back(k);
 }
 
@@ -323,6 +390,23 @@ cudaError_t exec_bluestein_tp(int prec, int64_t M, const void* src, void* dst, i
   p.inv_m = 1.0 / double(M);
   p.scale = scale;
   return k->run(p, -1, count, scratch, work, st);
+}
+
+cudaError_t exec_twopass_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
+                               int64_t rows, const void* tw1, const void* tw2, BigTwiddle bt, void* scratch,
+                               cudaStream_t st) {
+  cudaError_t e;
+  const BsTpKernel* k = bs_tp_ready(prec, M, &e);
+  if (!k) return e;
+  BsTpParams p{};
+  p.x = src;
+  p.out = dst;
+  p.items = items;
+  p.tw1 = tw1;
+  p.tw2 = tw2;
+  p.bt = bt;
+  p.inv_m = 1.0 / double(M);
+  return k->run_plain(p, dir, rows, scratch, st);
 }
 
 cudaError_t exec_bluestein_tp_items(int prec, int64_t M, int dir, const void* src, void* dst, const BigItem* items,
