@@ -170,6 +170,16 @@ struct GlobalStore {
   }
 };
 
+// This transform's padded row in shared memory as the first stage's input
+// and the last stage's output (the CTA stages global I/O itself).
+template <typename C, int N, int EPT>
+struct RowShared {
+  static constexpr bool kShared = true;
+  C* sh;
+  __device__ __forceinline__ C operator()(int e) const { return sh[Pow2Shape<N, EPT, sizeof(C)>::pad(e)]; }
+  __device__ __forceinline__ void operator()(int e, C x) const { sh[Pow2Shape<N, EPT, sizeof(C)>::pad(e)] = x; }
+};
+
 // Batched C2C: transform b reads src[b*idist .. b*idist+N) and writes
 // dst[b*odist ..).  src may equal dst (every CTA reads its whole transform
 // before it writes any of it).  tw holds W_N^m, m < N.
@@ -190,6 +200,33 @@ k_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, const 
   const int t = threadIdx.x % S::T;
   const int64_t b = int64_t(blockIdx.x) * S::B + threadIdx.x / S::T;
   const bool valid = b < count;
+  // Few threads per transform (rows of under 128 bytes per thread group):
+  // a direct load would touch short runs, so a contiguous batch is staged
+  // through shared memory, the CTA's B transforms read and written as one
+  // run with consecutive threads on consecutive elements.
+  if constexpr (S::T * int(sizeof(C)) < 128 && S::B > 1 && S::SMEM > 0) {
+    if (idist == N && odist == N) {
+      const int64_t b0 = int64_t(blockIdx.x) * S::B;
+      const int nb = int(count - b0 < S::B ? count - b0 : S::B);
+      C* shc = reinterpret_cast<C*>(smem_raw);
+      constexpr int LN = N == 1 ? 0 : (N == 2 ? 1 : (N == 4 ? 2 : (N == 8 ? 3 : (N == 16 ? 4 : (N == 32 ? 5 : (N == 64 ? 6 : (N == 128 ? 7 : 8)))))));
+      static_assert((1 << LN) == N, "staged I/O covers N <= 256");
+      const C* in = src + b0 * N;
+      for (int e = threadIdx.x; e < nb * N; e += S::TPB)
+        shc[(e >> LN) * S::STRIDE + S::pad(e & (N - 1))] = ld_stream(in + e);
+      __syncthreads();
+      RowShared<C, N, EPT> io{sh};
+      pow2_fft<C, N, EPT, DIR>(sh, t, tw, io, io);
+      __syncthreads();
+      C* out = dst + b0 * N;
+      for (int e = threadIdx.x; e < nb * N; e += S::TPB) {
+        C y = shc[(e >> LN) * S::STRIDE + S::pad(e & (N - 1))];
+        if constexpr (DIR > 0) y = cscale(y, scale);
+        st_stream(out + e, y);
+      }
+      return;
+    }
+  }
   GlobalLoad<C> ld{src + (valid ? b * idist : 0), valid};
   GlobalStore<C, (DIR > 0)> st{dst + (valid ? b * odist : 0), valid, scale};
   pow2_fft<C, N, EPT, DIR>(sh, t, tw, ld, st);

@@ -228,11 +228,12 @@ def test_large_in_place_and_many_groups(n):
     assert rel_l2(got, ref) <= tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n", [64, 1024, 8192, 16384, 2 ** 15, 2 ** 16, 2 ** 17, 2 ** 20, 2 ** 22, 2 ** 24])
+@pytest.mark.parametrize("n", [4, 16, 32, 64, 128, 1024, 8192, 16384, 2 ** 15, 2 ** 16, 2 ** 17, 2 ** 20, 2 ** 22, 2 ** 24])
 def test_every_variant_matches_oracle(n):
-    count = max(2, (1 << 20) // n)
+    count = max(2, (1 << 20) // n) + 3  # a partial last CTA for the batched kernels
     x = seeded_complex(n * count, seed=3 + n % 101)
     ref = O.batch(x[: 2 * n].astype(np.complex128), n)
+    ref_tail = O.batch(x[-2 * n:].astype(np.complex128), n)
     toks = algofft.Variants(n)
     assert toks
     for tok in toks:
@@ -242,6 +243,7 @@ def test_every_variant_matches_oracle(n):
             back = _run(p, y, count, inverse=True)
             p.Check()
         assert rel_l2(y[: 2 * n], ref) <= tol_c2c(n, False), tok
+        assert rel_l2(y[-2 * n:], ref_tail) <= tol_c2c(n, False), tok
         assert rel_l2(back, x) <= 2 * tol_c2c(n, False), tok
 
 
