@@ -64,10 +64,16 @@ k_r2c_pow2(const C* src, C* dst, int64_t count, int64_t idist, int64_t odist, co
   if (!valid) return;
   C* out = dst + b * odist;
   const C y0 = sh[0];
-  for (int k = t; k <= H; k += S::T) {
-    const C yk = k < H ? sh[S::pad(k)] : C{0, 0};
-    const C yhk = (k > 0 && k < H) ? sh[S::pad(H - k)] : C{0, 0};
+  if (t == 0) {
+    st_stream(out, cscale(r2c_bin(y0, y0, y0, C{0, 0}, 0, H), scale));
+    st_stream(out + H, cscale(r2c_bin(y0, y0, y0, C{0, 0}, H, H), scale));
+  }
+  // bins k and H - k share their two inputs: one pair of shared loads per
+  // two outputs, stored as an ascending and a descending run
+  for (int k = 1 + t; 2 * k <= H; k += S::T) {
+    const C yk = sh[S::pad(k)], yhk = sh[S::pad(H - k)];
     st_stream(out + k, cscale(r2c_bin(y0, yk, yhk, __ldg(wt + k), k, H), scale));
+    if (2 * k < H) st_stream(out + (H - k), cscale(r2c_bin(y0, yhk, yk, __ldg(wt + (H - k)), H - k, H), scale));
   }
 }
 
