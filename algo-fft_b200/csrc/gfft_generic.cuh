@@ -150,8 +150,10 @@ __device__ __forceinline__ void gen_fft_io(C* a, C* b, const C* gin, C* gout, ty
 // With ahead > 0 each CTA first asks the copy engine to bring the input of
 // CTA blockIdx + ahead into L2 (ahead = the co-resident CTAs), so loads
 // find it there about one CTA lifetime later.
-template <typename C, int DIR>
-__global__ void __launch_bounds__(1024) k_generic(const C* src, C* dst, int64_t count, int64_t idist,
+// LB bounds the CTA size: complex128 CTAs of up to 512 threads are compiled
+// for 128 registers (at 64 a radix-16 stage's 32 doubles spill).
+template <typename C, int DIR, int LB = 1024>
+__global__ void __launch_bounds__(LB) k_generic(const C* src, C* dst, int64_t count, int64_t idist,
                                                   int64_t odist, const C* __restrict__ tw, GenSched s,
                                                   typename RealOf<C>::type scale, int64_t ahead) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

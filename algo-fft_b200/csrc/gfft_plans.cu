@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 #include "gfft_generic.cuh"
 #include "gfft_internal.h"
@@ -95,21 +96,31 @@ static cudaError_t launch_generic(const PlanCore* c, int dir, const void* src, v
   const size_t smem = size_t(s.B) * s.stride * sizeof(C);
   const Re scale = Re(1.0 / double(c->n));
   // co-resident CTAs: the L2 prefetch distance (none for a single wave)
-  int dev = 0, sms = 0, occ = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, &k_generic<C, -1>, s.B * s.T, smem);
-  cudaGetLastError();
-  const int64_t resident = int64_t(sms) * std::max(occ, 1);
-  const int64_t ahead = blocks > resident ? resident : 0;
-  if (dir < 0)
-    k_generic<C, -1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
-                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale,
-                                                                  ahead);
-  else
-    k_generic<C, +1><<<unsigned(blocks), s.B * s.T, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst), count,
-                                                                  idist, odist, static_cast<const C*>(c->tw), s, scale,
-                                                                  ahead);
+  const int thr = s.B * s.T;
+  auto go = [&](auto lb) {
+    constexpr int LB = decltype(lb)::value;
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, &k_generic<C, -1, LB>, thr, smem);
+    cudaGetLastError();
+    const int64_t resident = int64_t(sms) * std::max(occ, 1);
+    const int64_t ahead = blocks > resident ? resident : 0;
+    if (dir < 0)
+      k_generic<C, -1, LB><<<unsigned(blocks), thr, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst),
+                                                                  count, idist, odist, static_cast<const C*>(c->tw), s,
+                                                                  scale, ahead);
+    else
+      k_generic<C, +1, LB><<<unsigned(blocks), thr, smem, st>>>(static_cast<const C*>(src), static_cast<C*>(dst),
+                                                                  count, idist, odist, static_cast<const C*>(c->tw), s,
+                                                                  scale, ahead);
+  };
+  if constexpr (sizeof(C) == 16) {
+    if (thr <= 512) go(std::integral_constant<int, 512>{});
+    else go(std::integral_constant<int, 1024>{});
+  } else {
+    go(std::integral_constant<int, 1024>{});
+  }
   return cudaGetLastError();
 }
 
@@ -147,6 +158,8 @@ static cudaError_t prepare_generic_kernels() {
       reinterpret_cast<const void*>(&k_generic<float2, +1>),
       reinterpret_cast<const void*>(&k_generic<double2, -1>),
       reinterpret_cast<const void*>(&k_generic<double2, +1>),
+      reinterpret_cast<const void*>(&k_generic<double2, -1, 512>),
+      reinterpret_cast<const void*>(&k_generic<double2, +1, 512>),
       reinterpret_cast<const void*>(&k_gen_cols<float2, -1, GEN_PASS1>),
       reinterpret_cast<const void*>(&k_gen_cols<float2, +1, GEN_PASS1>),
       reinterpret_cast<const void*>(&k_gen_cols<float2, -1, GEN_PASS2>),
