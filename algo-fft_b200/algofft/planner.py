@@ -6,7 +6,7 @@ The cost model scores (shape, variant) pairs (features: gfft_planner_features)
 with a predicted log(ns per element); plan creation with
 ``PlanOptions(Planner=PlannerLearned)`` takes the variant with the smallest
 prediction when the wisdom store has no entry.  Exhaustive measurement (the
-autotuner) is the fallback and the judge: regret = time of the chosen variant
+autotuner) is the fallback and the arbiter: regret = time of the chosen variant
 / time of the fastest measured one.
 
     python -m algofft.planner collect --count 3500 --out DATA.jsonl   # on a GPU

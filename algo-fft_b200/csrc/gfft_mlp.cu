@@ -11,7 +11,7 @@
 // Plan creation with GFFT_PLANNER_LEARNED evaluates every candidate of the
 // length in one inference launch and takes the smallest prediction; the
 // wisdom store still wins where it has an entry, and exhaustive measurement
-// (GFFT_PLANNER_MEASURE and up, the autotuner) stays the judge the model is
+// (GFFT_PLANNER_MEASURE and up, the autotuner) stays the arbiter the model is
 // trained on and scored against.  The reference decides by size class alone
 // (internal/planner/planner.go:43-78, selection.go:66-108) and measures per
 // size (internal/fft/measure.go:89-228); it has no learned model.

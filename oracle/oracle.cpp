@@ -3,7 +3,7 @@
 // This file is the checker: it is linked by the tests, by the smoke check
 // and by the CPU-baseline leg of the benchmark, never by the product
 // library.  It restates, in C++, the reference's CPU algorithms for the path
-// (CWBudde/algo-fft, pure-Go build) plus an FP64 naive DFT judge.  Each
+// (CWBudde/algo-fft, pure-Go build) plus an FP64 naive DFT arbiter.  Each
 // function cites the reference file:line it follows.
 //
 // Parity pinning: the reference is Go and no Go toolchain exists on either
@@ -472,7 +472,7 @@ int real_inverse(R* dst, const cx<R>* src, int64_t n) {
 
 extern "C" {
 
-// FP64 naive DFT, the judge.  Follows internal/reference/dft.go:16-150
+// FP64 naive DFT, the arbiter.  Follows internal/reference/dft.go:16-150
 // (NaiveDFT128/NaiveIDFT128: sum x[j] exp(∓2πi jk/n), inverse * 1/n) but
 // reduces the angle exactly as (j*k mod n) before the float64 evaluation,
 // so its angles are within 1 ulp of the exact ones for every n.
@@ -506,7 +506,7 @@ void orc_naive_dft_f64(const double* in, double* out, int64_t n, int inverse) {
 
 // internal/reference/dft.go:16-51 NaiveDFT / :61-96 NaiveIDFT verbatim
 // formula (angle = ∓2π·k·j/n in float64 without reduction), complex128
-// accumulation, used to pin the judge against the reference's own oracle.
+// accumulation, used to pin the arbiter against the reference's own oracle.
 void orc_naive_dft_ref(const double* in, double* out, int64_t n, int inverse) {
   const auto* x = reinterpret_cast<const cx<double>*>(in);
   auto* y = reinterpret_cast<cx<double>*>(out);

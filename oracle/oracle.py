@@ -66,7 +66,7 @@ def _p(a: np.ndarray):
 
 
 def naive_dft(x: np.ndarray, inverse: bool = False) -> np.ndarray:
-    """FP64 judge (exact angle reduction); returns complex128."""
+    """FP64 arbiter (exact angle reduction); returns complex128."""
     x = np.ascontiguousarray(x, dtype=np.complex128)
     y = np.empty_like(x)
     lib().orc_naive_dft_f64(_p(x), _p(y), x.size, int(inverse))

@@ -22,7 +22,7 @@ def _torch():
 
 
 def _fp64_reference(x: np.ndarray, n: int, inverse=False) -> np.ndarray:
-    """FP64 judge: the naive DFT for small n, else the oracle's complex128
+    """FP64 arbiter: the naive DFT for small n, else the oracle's complex128
     FFT (itself checked against the naive DFT on the CPU)."""
     x64 = x.astype(np.complex128)
     if n <= 512:

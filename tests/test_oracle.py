@@ -22,7 +22,7 @@ def test_oracle_c2c_known_answers(case):
     x = _cx(case["input"], dtype)
     want = _cx(case["expected"], np.complex128)
     inv = case["kind"] == "inverse"
-    # the FP64 judge
+    # the FP64 arbiter
     got = O.naive_dft(x, inverse=inv)
     assert np.max(np.abs(got - want)) <= case["tol"]
     # the reference's own NaiveDFT formula

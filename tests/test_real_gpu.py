@@ -1,5 +1,5 @@
 """Parity of the real-input path (PlanReal Forward/Inverse,
-plan_real_generic.go) with the oracle and the FP64 judge."""
+plan_real_generic.go) with the oracle and the FP64 arbiter."""
 import json
 import os
 
