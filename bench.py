@@ -83,58 +83,133 @@ def tensor_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while timing."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled while timing, each sample
+    stamped with the host's monotonic time so that summary() keeps the ones
+    inside the timed window.  NVML is polled every 10 ms by a thread
+    (read-only queries); without NVML, nvidia-smi reports every 200 ms."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    SMI_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
-        self.index = index
-        self.rows = []
+    def __init__(self, index: int, pci_bus_id: str | None = None, period_s: float = 0.01):
+        self.index, self.pci_bus_id, self.period_s = index, pci_bus_id, period_s
+        self.rows = []          # (host time, sm MHz, max sm MHz, set of active reason names)
+        self.source = None
         self._p = None
+        self._stop = threading.Event()
+        self._t = None
 
     def __enter__(self):
-        try:
-            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                        "--format=csv,noheader,nounits", "-lms", "200"],
-                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-            t0 = time.time()
-            while not self.rows and time.time() - t0 < 5.0 and self._p.poll() is None:
-                time.sleep(0.05)
-        except Exception:
-            self._p = None
+        if not self._start_nvml():
+            self._start_smi()
+        t0 = time.monotonic()
+        while not self.rows and time.monotonic() - t0 < 5.0 and self._t is not None and self._t.is_alive():
+            time.sleep(0.01)
         return self
 
-    def mark(self):
-        """Index of the first sample taken after this call."""
-        return len(self.rows)
+    def _start_nvml(self) -> bool:
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            if self.pci_bus_id:
+                try:
+                    h = nv.nvmlDeviceGetHandleByPciBusId(self.pci_bus_id)
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            suffix = ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")
+            bits = [getattr(nv, "nvmlClocksEventReason" + x, None) or getattr(nv, "nvmlClocksThrottleReason" + x)
+                    for x in suffix]
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            get_reasons(h)
+        except Exception:
+            return False
 
-    def _read(self):
-        for line in self._p.stdout:
-            parts = [s.strip() for s in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+        def poll():
+            while not self._stop.is_set():
+                try:
+                    t = time.monotonic()
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = int(get_reasons(h))
+                except Exception:
+                    return
+                self.rows.append((t, sm, mx, {self.NAMES[i] for i in range(4) if r & bits[i]}))
+                self._stop.wait(self.period_s)
+
+        self.source = f"nvml every {self.period_s * 1e3:g} ms"
+        self._t = threading.Thread(target=poll, daemon=True)
+        self._t.start()
+        return True
+
+    def _start_smi(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.SMI_Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
+            return
+
+        def read():
+            for line in self._p.stdout:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                num = [float(v) if v.replace(".", "").isdigit() else None for v in parts[1:3]]
+                if num[0] is None:
+                    continue
+                self.rows.append((time.monotonic(), num[0], num[1],
+                                  {self.NAMES[i] for i in range(4) if parts[5 + i].lower() == "active"}))
+
+        self.source = "nvidia-smi every 200 ms"
+        self._t = threading.Thread(target=read, daemon=True)
+        self._t.start()
+
+    def mark(self) -> float:
+        """Host time; samples taken after it belong to the window."""
+        return time.monotonic()
 
     def __exit__(self, *a):
+        self._stop.set()
         if self._p:
             self._p.terminate()
             try:
                 self._p.wait(timeout=5)
             except Exception:
                 self._p.kill()
+        if self._t is not None:
+            self._t.join(timeout=1.0)
 
-    def summary(self, since: int = 0):
-        rows = self.rows[since:] or self.rows
+    def summary(self, t0: float = float("-inf"), t1: float = float("inf")):
+        """Median SM clock, max clock and the union of active reasons over the
+        samples taken in [t0, t1]; when the window is shorter than the
+        sampling period, the first sample after t0."""
+        rows = [r for r in self.rows if t0 <= r[0] <= t1]
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            rows = [r for r in self.rows if r[0] >= t0][:1] or self.rows[-1:]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "source": self.source}
+        mx = [r[2] for r in rows if r[2] is not None]
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(set().union(*(r[3] for r in rows))), "samples": len(rows),
+                "source": self.source}
+
+
+def pci_bus_id(dev) -> str | None:
+    """NVML bus id ("domain:bus:device.0") of a torch CUDA device."""
+    try:
+        import torch
+        pr = torch.cuda.get_device_properties(dev)
+        return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        return None
 
 
 def shard(count: int, rank: int, world: int) -> tuple[int, int]:
@@ -504,7 +579,7 @@ def main():
             if evs is not None:
                 evs[i].record(stream)
 
-    clk = ClockSampler(local).__enter__()
+    clk = ClockSampler(local, pci_bus_id(dev)).__enter__()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -525,8 +600,9 @@ def main():
             per_size_ms[n] += prev.elapsed_time(evs[i])
             prev = evs[i]
     torch.cuda.synchronize()
-    time.sleep(0.3)
-    clocks = clk.summary(mark)
+    mark_end = clk.mark()
+    time.sleep(0.25)
+    clocks = clk.summary(mark, mark_end)
     dev_ms = max_over_ranks(sum(per_size_ms.values()), pg, dev)  # device time of the K steps
     bytes_step = sum(bytes_per_transform(n) * bufs[n][2] for n in SWEEP)
     value = world * bytes_step * args.steps / (dev_ms / 1e3) / 1e9
