@@ -231,16 +231,25 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
     const C* lo = static_cast<const C*>(bt.lo);
     const C* hi = static_cast<const C*>(bt.hi);
     const int64_t mask = (int64_t(1) << bt.shift) - 1;
-    // column by column, rows k1 across the threads (runs of L in HBM)
-    for (int c = 0; c < NC; ++c) {
-      const int64_t n2 = col0 + c;
-      if (n2 >= ncols) break;
-      const C* rc = res + c * s.stride;
-      for (int k1 = tid; k1 < L; k1 += nthr) {
-        const int64_t m = n2 * k1;
-        C w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
-        if constexpr (DIR > 0) w.y = -w.y;
-        __stcg(out + n2 * L + k1, cmul(rc[gpad(k1)], w));
+    // rows k1 across the threads (each store instruction writes a run of
+    // the row n2 in HBM), columns in turn; W^(n2 k1) of the next column is
+    // this one's times W^(k1) (a coalesced lookup), gathered exactly every
+    // fourth column so rounding grows by at most three products
+    for (int k1 = tid; k1 < L; k1 += nthr) {
+      const C step = cmul(__ldg(hi + (k1 >> bt.shift)), __ldg(lo + (k1 & mask)));
+      C w = C{1, 0};
+      for (int c = 0; c < NC; ++c) {
+        const int64_t n2 = col0 + c;
+        if (n2 >= ncols) break;
+        if ((c & 3) == 0) {
+          const int64_t m = n2 * k1;
+          w = cmul(__ldg(hi + (m >> bt.shift)), __ldg(lo + (m & mask)));
+        } else {
+          w = cmul(w, step);
+        }
+        C wd = w;
+        if constexpr (DIR > 0) wd.y = -wd.y;
+        __stcg(out + n2 * L + k1, cmul(res[c * s.stride + gpad(k1)], wd));
       }
     }
   } else {
