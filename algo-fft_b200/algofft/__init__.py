@@ -12,6 +12,7 @@ from .plan import (COMPLEX64, COMPLEX128, Executor, GetKernelStrategy, KernelAut
                    PlanOptions, PlannerEstimate, RecordBenchmarkDecision, SetKernelStrategy, PlannerExhaustive, PlannerLearned, PlannerMeasure,
                    PlannerPatient)
 
+from .distributed import PlanDistributed
 from .convolve import (AutoCorrelate, AutoCorrelate128, Convolve, Convolve128, ConvolveReal, ConvolveRealBatch,
                        Correlate, Correlate128, CrossCorrelate, CrossCorrelate128)
 from .nd import NewPlan2D, NewPlan3D, NewPlanND, NewPlanReal2D, NewPlanReal3D, PlanND
