@@ -81,6 +81,12 @@ class PlanDistributed:
         ang = m.to(torch.float64) * (-2.0 * math.pi / self.n)
         self.twiddle = torch.polar(torch.ones_like(ang), ang).to(self.dtype).to(self.device)
 
+    def _tw(self, device, inverse: bool):
+        """The twiddle table on the slabs' device (moved there once)."""
+        if self.twiddle.device != device:
+            self.twiddle = self.twiddle.to(device)
+        return self.twiddle.conj() if inverse else self.twiddle
+
     # -- local pieces --------------------------------------------------------
 
     def _device_fft(self, x, inverse: bool):
@@ -118,7 +124,7 @@ class PlanDistributed:
         """Steps 1-4 from this rank's natural slab."""
         P, N1, N2 = self.world, self.n1, self.n2
         r1, r2 = N1 // P, N2 // P
-        tw = self.twiddle.conj() if inverse else self.twiddle
+        tw = self._tw(x.device, inverse)
         # rows n1 of this rank (r1 x N2) -> columns n2 of this rank (N1 x r2)
         a = x.reshape(r1, P, r2).permute(1, 0, 2)
         cols = self._exchange(a).reshape(N1, r2)
@@ -141,7 +147,7 @@ class PlanDistributed:
         P, N1, N2 = self.world, self.n1, self.n2
         r1, r2 = N1 // P, N2 // P
         inverse = True
-        tw = self.twiddle.conj()
+        tw = self._tw(z.device, True)
         # transforms over k2 of the rank's k1 rows
         y = self._local_fft(z.contiguous(), inverse)                           # (r1 k1, N2 n2)
         b = y.reshape(r1, P, r2).permute(1, 0, 2)                              # block q: n2 of rank q
