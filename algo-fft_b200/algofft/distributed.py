@@ -90,12 +90,17 @@ class PlanDistributed:
     # -- local pieces --------------------------------------------------------
 
     def _device_fft(self, x, inverse: bool):
-        from .plan import Plan
+        """The library's batched transform of the rows of x, by a plan on x's
+        own device (one plan per (length, device))."""
+        from .plan import Plan, PlanOptions
         import torch
+        if not x.is_cuda:
+            raise ValueError("the default local transform needs slabs on a CUDA device")
         count, length = x.shape
-        key = length
+        dev = x.device.index if x.device.index is not None else torch.cuda.current_device()
+        key = (length, dev)
         if key not in self._plans:
-            self._plans[key] = Plan(length, self.precision)
+            self._plans[key] = Plan(length, self.precision, PlanOptions(Device=dev))
         out = torch.empty_like(x)
         p = self._plans[key]
         (p.InverseBatch if inverse else p.ForwardBatch)(out, x, count)

@@ -30,50 +30,6 @@ gfft_status cuda_status(cudaError_t e, const char* what) {
 
 static cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
-// Host-slice path: the batch moves in chunks of about 64 MB through three
-// streams and three staging buffers (workspace pool): chunk k's copy in, its
-// transforms and its copy out are ordered on stream k % 3, so the copy out
-// of one chunk, the transforms of the next and the copy in of the one
-// after run at once (both directions of the host link busy, transforms
-// hidden under the copies).  With pageable host memory the copies still
-// complete correctly but cannot overlap.  Returns after the last copy out.
-static gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count) {
-  constexpr int kLanes = 3;
-  const size_t tb = size_t(p->core.n) * elem_bytes(p->core.prec);
-  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(count, int64_t((size_t(64) << 20) / tb)));
-  cudaStream_t st[kLanes] = {};
-  void* d[kLanes] = {};
-  gfft_status s = GFFT_OK;
-  cudaError_t e = cudaSuccess;
-  for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
-  for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = ws_alloc(&d[i], size_t(per) * tb, st[i]);
-  if (e != cudaSuccess) s = cuda_status(e, "host path setup");
-  int k = 0;
-  for (int64_t b0 = 0; b0 < count && s == GFFT_OK; b0 += per, ++k) {
-    const int64_t m = std::min(per, count - b0);
-    const size_t bytes = size_t(m) * tb, off = size_t(b0) * tb;
-    cudaStream_t q = st[k % kLanes];
-    void* buf = d[k % kLanes];
-    e = cudaMemcpyAsync(buf, static_cast<const char*>(src) + off, bytes, cudaMemcpyHostToDevice, q);
-    if (e != cudaSuccess) {
-      s = cuda_status(e, "cudaMemcpyAsync(H2D)");
-      break;
-    }
-    s = core_exec(&p->core, dir, buf, buf, m, p->core.n, p->core.n, q);
-    if (s != GFFT_OK) break;
-    e = cudaMemcpyAsync(static_cast<char*>(dst) + off, buf, bytes, cudaMemcpyDeviceToHost, q);
-    if (e != cudaSuccess) s = cuda_status(e, "cudaMemcpyAsync(D2H)");
-  }
-  for (int i = 0; i < kLanes; ++i) {
-    if (!st[i]) continue;
-    if (d[i]) cudaFreeAsync(d[i], st[i]);
-    e = cudaStreamSynchronize(st[i]);
-    if (e != cudaSuccess && s == GFFT_OK) s = cuda_status(e, "cudaStreamSynchronize");
-    cudaStreamDestroy(st[i]);
-  }
-  return s;
-}
-
 }  // namespace gfft
 
 using namespace gfft;
@@ -98,7 +54,8 @@ gfft_status gfft_plan_new(gfft_plan** out, int32_t precision, int64_t n, const g
     return GFFT_ERR_NO_DEVICE;
   }
   if (o.device < 0 || o.device >= ndev) return GFFT_ERR_INVALID_ARGUMENT;
-  GFFT_CUDA(cudaSetDevice(o.device));
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(o.device));
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts = o;
@@ -201,7 +158,8 @@ gfft_status gfft_plan_clone(gfft_plan** out, const gfft_plan* src) {
   clear_error();
   if (!out || !src) return GFFT_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  GFFT_CUDA(cudaSetDevice(src->core.device));
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(src->core.device));
   auto* p = new (std::nothrow) gfft_plan;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->opts = src->opts;
@@ -253,6 +211,8 @@ static gfft_status do_single(gfft_plan* p, int dir, void* dst, int64_t dst_len, 
   clear_error();
   gfft_status s = check_single(p, dst, dst_len, src, src_len);
   if (s != GFFT_OK) return s;
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->core.device));
   return core_exec(&p->core, dir, dst, src, 1, p->core.n, p->core.n, as_stream(stream));
 }
 
@@ -261,6 +221,8 @@ static gfft_status do_batch(gfft_plan* p, int dir, void* dst, int64_t dst_len, c
   clear_error();
   gfft_status s = check_batch(p, dst, dst_len, src, src_len, count);
   if (s != GFFT_OK) return s;
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->core.device));
   return core_exec(&p->core, dir, dst, src, count, p->core.n, p->core.n, as_stream(stream));
 }
 
@@ -302,6 +264,8 @@ static gfft_status do_strided(gfft_plan* p, int dir, void* dst, int64_t dst_len,
   clear_error();
   gfft_status s = check_strided(p, dst, dst_len, src, src_len, stride);
   if (s != GFFT_OK) return s;
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->core.device));
   const int64_t n = p->core.n;
   if (stride == 1) return core_exec(&p->core, dir, dst, src, 1, n, n, as_stream(stream));
   // Gather the column into a contiguous buffer, transform, scatter back

@@ -1,0 +1,226 @@
+// Host-slice execution of 1-D batches (the Go-slice methods Plan.Forward /
+// ForwardBatch with []complex64 arguments, plan.go:332-571).
+//
+// A Go slice lives in pageable memory, which the copy engines cannot read
+// directly: the driver then copies through its own small staging area and
+// the copies of one call neither overlap each other nor the transforms.  So
+// a batch in pageable memory moves through library-owned pinned lanes:
+//   host thread pool: pageable src chunk -> pinned lane buffer
+//   lane stream:      pinned -> device, transforms, device -> pinned
+//   host thread pool: pinned lane buffer -> pageable dst chunk
+// with three lanes in flight, so the host copies of one chunk overlap the
+// device copies and transforms of the other two.  Buffers that are already
+// pinned (cudaHostAlloc / cudaHostRegister) skip the host copies and go
+// straight through the lanes' device buffers.
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+#include "gfft_internal.h"
+
+namespace gfft {
+namespace {
+
+// Splits large memcpys over a few persistent threads (one call at a time;
+// the calling thread takes a share too).
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool* pool = new CopyPool();  // never destroyed: workers outlive static teardown
+    return *pool;
+  }
+
+  void copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPart = size_t(1) << 20;
+    if (bytes <= 2 * kPart || workers_.empty()) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    std::lock_guard<std::mutex> one(call_mu_);
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      dst_ = static_cast<char*>(dst);
+      src_ = static_cast<const char*>(src);
+      bytes_ = bytes;
+      part_ = std::max(kPart, (bytes / (workers_.size() + 1) + 4095) & ~size_t(4095));
+      next_.store(0);
+      busy_ = workers_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    run_parts();
+    std::unique_lock<std::mutex> g(mu_);
+    done_cv_.wait(g, [&] { return busy_ == 0; });
+  }
+
+ private:
+  CopyPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned n = std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+    for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    for (auto& t : workers_) t.detach();
+  }
+
+  void run_parts() {
+    for (;;) {
+      const size_t at = next_.fetch_add(part_);
+      if (at >= bytes_) return;
+      std::memcpy(dst_ + at, src_ + at, std::min(part_, bytes_ - at));
+    }
+  }
+
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      run_parts();
+      std::lock_guard<std::mutex> g(mu_);
+      if (--busy_ == 0) done_cv_.notify_all();
+    }
+  }
+
+  std::vector<std::thread> workers_;
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t bytes_ = 0, part_ = 0, busy_ = 0;
+  std::atomic<size_t> next_{0};
+  uint64_t gen_ = 0;
+};
+
+// Pinned staging buffers kept for later calls (portable: any device may
+// copy from them); one lane set per concurrent call.
+class PinnedPool {
+ public:
+  static PinnedPool& get() {
+    static PinnedPool* pool = new PinnedPool();
+    return *pool;
+  }
+  cudaError_t acquire(size_t bytes, void** out) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first <= 2 * bytes) {
+        *out = it->second;
+        free_.erase(it);
+        return cudaSuccess;
+      }
+    }
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e == cudaSuccess) {
+      std::lock_guard<std::mutex> g(mu_);
+      size_of_[*out] = bytes;
+    }
+    return e;
+  }
+  void release(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(mu_);
+    free_.emplace(size_of_[p], p);
+  }
+
+ private:
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  std::map<void*, size_t> size_of_;
+};
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // older drivers report unregistered memory as an error
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+constexpr int kLanes = 3;
+
+}  // namespace
+
+gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count) {
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->core.device));
+  const size_t tb = size_t(p->core.n) * elem_bytes(p->core.prec);
+  const bool staged = !(host_pinned(src) && host_pinned(dst));
+  // chunks of about 64 MB (pinned) / 32 MB (staged), whole transforms
+  const size_t target = staged ? (size_t(32) << 20) : (size_t(64) << 20);
+  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(count, int64_t(target / tb)));
+  const int64_t nchunks = (count + per - 1) / per;
+  const int lanes = int(std::min<int64_t>(kLanes, nchunks));
+  cudaStream_t st[kLanes] = {};
+  cudaEvent_t ev[kLanes] = {};
+  void* d[kLanes] = {};
+  void* h[kLanes] = {};
+  int64_t pending[kLanes] = {-1, -1, -1};  // chunk whose result waits in lane's pinned buffer
+  gfft_status s = GFFT_OK;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
+  for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+  for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = ws_alloc(&d[i], size_t(per) * tb, st[i]);
+  for (int i = 0; staged && i < lanes && e == cudaSuccess; ++i) e = PinnedPool::get().acquire(size_t(per) * tb, &h[i]);
+  if (e != cudaSuccess) s = cuda_status(e, "host path setup");
+  CopyPool& cp = CopyPool::get();
+  auto chunk_bytes = [&](int64_t k) { return size_t(std::min(per, count - k * per)) * tb; };
+  // copies a finished chunk from its lane's pinned buffer to dst
+  auto drain = [&](int lane) -> gfft_status {
+    if (pending[lane] < 0) return GFFT_OK;
+    const int64_t k = pending[lane];
+    pending[lane] = -1;
+    cudaError_t ee = cudaEventSynchronize(ev[lane]);
+    if (ee != cudaSuccess) return cuda_status(ee, "cudaEventSynchronize");
+    cp.copy(static_cast<char*>(dst) + size_t(k * per) * tb, h[lane], chunk_bytes(k));
+    return GFFT_OK;
+  };
+  for (int64_t k = 0; k < nchunks && s == GFFT_OK; ++k) {
+    const int lane = int(k % lanes);
+    const size_t bytes = chunk_bytes(k), off = size_t(k * per) * tb;
+    const int64_t m = int64_t(bytes / tb);
+    const void* in = static_cast<const char*>(src) + off;
+    void* out = static_cast<char*>(dst) + off;
+    if (staged) {
+      s = drain(lane);
+      if (s != GFFT_OK) break;
+      cp.copy(h[lane], in, bytes);
+      in = h[lane];
+      out = h[lane];
+    }
+    e = cudaMemcpyAsync(d[lane], in, bytes, cudaMemcpyHostToDevice, st[lane]);
+    if (e != cudaSuccess) {
+      s = cuda_status(e, "cudaMemcpyAsync(H2D)");
+      break;
+    }
+    s = core_exec(&p->core, dir, d[lane], d[lane], m, p->core.n, p->core.n, st[lane]);
+    if (s != GFFT_OK) break;
+    e = cudaMemcpyAsync(out, d[lane], bytes, cudaMemcpyDeviceToHost, st[lane]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[lane], st[lane]);
+    if (e != cudaSuccess) {
+      s = cuda_status(e, "cudaMemcpyAsync(D2H)");
+      break;
+    }
+    if (staged) pending[lane] = k;
+  }
+  // results of the last chunks, oldest first
+  for (int64_t k = std::max<int64_t>(0, nchunks - lanes); k < nchunks && s == GFFT_OK; ++k) s = drain(int(k % lanes));
+  for (int i = 0; i < lanes; ++i) {
+    if (!st[i]) continue;
+    if (d[i]) cudaFreeAsync(d[i], st[i]);
+    e = cudaStreamSynchronize(st[i]);
+    if (e != cudaSuccess && s == GFFT_OK) s = cuda_status(e, "cudaStreamSynchronize");
+    cudaStreamDestroy(st[i]);
+    if (ev[i]) cudaEventDestroy(ev[i]);
+    PinnedPool::get().release(h[i]);
+  }
+  return s;
+}
+
+}  // namespace gfft

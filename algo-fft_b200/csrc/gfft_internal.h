@@ -21,6 +21,30 @@ gfft_status cuda_status(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::gfft::cuda_status(e_, #call); \
   } while (0)
 
+// Makes a device current for the guard's scope and gives the calling thread
+// its previous current device back when the scope ends, so no entry point
+// leaves the caller's device changed.
+class DeviceGuard {
+ public:
+  DeviceGuard() = default;
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+  cudaError_t set(int device) {
+    cudaError_t e = cudaGetDevice(&prev_);
+    if (e != cudaSuccess || prev_ == device) return e;
+    e = cudaSetDevice(device);
+    restore_ = e == cudaSuccess;
+    return e;
+  }
+  ~DeviceGuard() {
+    if (restore_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0;
+  bool restore_ = false;
+};
+
 enum class Algo { Trivial, Pow2Smem, TwoPass, ThreePass, Generic, GenTwoPass, Bluestein, TensorCore };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
@@ -166,6 +190,14 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
 
 inline size_t elem_bytes(int prec) { return prec == kC64 ? 8 : 16; }
 
+}  // namespace gfft
+
+struct gfft_plan;
+namespace gfft {
+// Host-slice execution of `count` transforms of a 1-D plan: copies in,
+// transforms and copies out before returning (pageable buffers are staged
+// through library-owned pinned lanes).
+gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count);
 }  // namespace gfft
 
 struct gfft_plan {

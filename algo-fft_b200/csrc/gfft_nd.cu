@@ -214,7 +214,9 @@ extern "C" gfft_status gfft_plan_nd_new(gfft_plan_nd** out, int32_t precision, i
   if (opts) o = *opts;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
-  GFFT_CUDA(cudaSetDevice(o.device));
+  if (o.device < 0 || o.device >= ndev) return GFFT_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(o.device));
   auto* p = new (std::nothrow) gfft_plan_nd;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->prec = precision;

@@ -14,12 +14,14 @@
 // Every GPU that loads libgfft.so holds it for the life of the process.
 // Host code only sees a host-side stand-in for its name, so the device
 // address is looked up once per device with cudaGetSymbolAddress (the first
-// call on each device does that, with the device current; make that first
-// call before any stream capture).  The region is shared by every call: the
-// tile counters at its start are cleared on the call's stream before the
-// kernel runs, the slots after them are fully written before they are read,
-// and two calls that overlap on the GPU (different streams, or a call still
-// running while another starts) race on it.
+// call on each device does that, with the plan's device current; make that
+// first call before any stream capture).  The region is shared by every
+// call: the call's abort word and tile counters at its start are cleared on
+// the call's stream before the kernel runs, the slots after them are fully
+// written before they are read, and two calls that overlap on the GPU
+// (different streams, or a call still running while another starts) race on
+// it.  A bounded wait that expires stops only the call it happened in; it
+// also sets the plan's sticky status word, which gfft_plan_check reports.
 #include <mutex>
 #include "gfft_internal.h"
 #include "gfft_twopass.cuh"
@@ -29,7 +31,8 @@ namespace gfft {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
-constexpr size_t kNoAllocCounterBytes = size_t(512) << 10;  // tile counter + per-group counters
+constexpr size_t kNoAllocCounterBytes = size_t(512) << 10;  // abort word, tile counter, per-group counters
+constexpr size_t kNoAllocStatusBytes = 256;                   // the abort word's own line at the start
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -38,7 +41,7 @@ std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the static scratch on the current device, looked up the
-// first time a device is seen.
+// first time a device is seen (the caller has made the plan's device current).
 gfft_status noalloc_scratch(void** out) {
   int dev = 0;
   GFFT_CUDA(cudaGetDevice(&dev));
@@ -91,16 +94,20 @@ extern "C" gfft_status gfft_exec_batch_noalloc(gfft_plan* plan, int32_t directio
   int64_t group = std::min<int64_t>(c->group, std::max<int64_t>(1, int64_t(slot_space / (2 * tbytes))));
   int64_t slots = std::max<int64_t>(2, std::min<int64_t>(c->slots, int64_t(slot_space / (group * tbytes))));
   const int64_t groups = (count + group - 1) / group;
-  if (size_t(1 + 2 * groups) * sizeof(unsigned) > kNoAllocCounterBytes) {
+  const size_t ctr_bytes = size_t(1 + 2 * groups) * sizeof(unsigned);
+  if (kNoAllocStatusBytes + ctr_bytes > kNoAllocCounterBytes) {
     set_error("batch of " + std::to_string(count) + " transforms needs more tile counters than the " +
               std::to_string(kNoAllocCounterBytes) + "-byte counter area of the no-allocation path holds");
     return GFFT_ERR_INVALID_ARGUMENT;
   }
+  // The scratch, twiddles and status word all live on the plan's device.
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(c->device));
   void* base = nullptr;
   gfft_status s = noalloc_scratch(&base);
   if (s != GFFT_OK) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  GFFT_CUDA(cudaMemsetAsync(base, 0, size_t(1 + 2 * groups) * sizeof(unsigned), st));
+  GFFT_CUDA(cudaMemsetAsync(base, 0, kNoAllocStatusBytes + ctr_bytes, st));
   const TwoPassKernel* k = c->tp[direction < 0 ? 0 : 1];
   TwoPassParams p;
   p.src = src;
@@ -114,8 +121,9 @@ extern "C" gfft_status gfft_exec_batch_noalloc(gfft_plan* plan, int32_t directio
   p.bt.lo = c->bt_lo;
   p.bt.hi = c->bt_hi;
   p.bt.shift = c->bt_shift;
-  p.ctr = static_cast<unsigned*>(base);
-  p.status = c->status;
+  p.ctr = reinterpret_cast<unsigned*>(static_cast<char*>(base) + kNoAllocStatusBytes);
+  p.status = static_cast<unsigned*>(base);
+  p.report = c->status;
   p.groups = int(groups);
   p.G = int(group);
   p.S = int(slots);

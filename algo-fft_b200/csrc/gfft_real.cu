@@ -143,7 +143,8 @@ gfft_status gfft_plan_real_new(gfft_plan_real** out, int32_t precision, int64_t 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
   if (o.device < 0 || o.device >= ndev) return GFFT_ERR_INVALID_ARGUMENT;
-  GFFT_CUDA(cudaSetDevice(o.device));
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(o.device));
   auto* p = new (std::nothrow) gfft_plan_real;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->prec = precision;

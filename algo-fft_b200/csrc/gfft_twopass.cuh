@@ -233,7 +233,8 @@ struct TwoPassParams {
   const void* tw2;     // W_N2^m, m < N2
   BigTwiddle bt;       // W_N^m
   unsigned* ctr;       // [0] next tile, [1 + g] pass-1 done, [1 + groups + g] pass-2 done
-  unsigned* status;    // 0 ok, 1 a bounded wait expired
+  unsigned* status;    // 0 ok, 1 a bounded wait expired (every CTA stops at its next tile)
+  unsigned* report = nullptr;  // optional sticky word also set when a wait expires (the plan's)
   int groups, G, S;
   double scale;        // applied in pass 2 (1/N for the inverse)
   unsigned spin_limit;
@@ -344,7 +345,10 @@ k_twopass(TwoPassParams p) {
       bool ok = true;
       if (pass == 2) ok = wait_at_least(done1 + g, unsigned(T1), p.spin_limit);
       else if (g >= p.S) ok = wait_at_least(done2 + (g - p.S), unsigned(T2), p.spin_limit);
-      if (!ok) atomicExch(p.status, 1u);
+      if (!ok) {
+        atomicExch(p.status, 1u);
+        if (p.report) atomicOr(p.report, 1u);
+      }
       s_ok = ok;
     }
     __syncthreads();

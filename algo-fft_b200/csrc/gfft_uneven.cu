@@ -93,10 +93,39 @@ struct gfft_plan_uneven {
     const void* src;
     void* dst;
     cudaGraphExec_t exec;
+    uint64_t used;  // call tick of the last replay (least recently used goes first)
   };
   std::vector<Graph> graphs;
+  uint64_t tick = 0;
   cudaStream_t cap = nullptr;
+  // Recorded after every call's work: the next call, on whatever stream,
+  // waits for it, so calls on one plan never overlap on the device (they
+  // share the work buffers and queue counters above).
+  cudaEvent_t done = nullptr;
 };
+
+namespace {
+constexpr size_t kMaxGraphs = 8;  // instantiated graphs kept per plan
+
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Orders this call after the plan's previous one (skipped while the caller
+// captures `st` into its own graph: the capture orders its replays).
+gfft_status after_previous_call(gfft_plan_uneven* p, cudaStream_t st) {
+  if (capturing(st)) return GFFT_OK;
+  GFFT_CUDA(cudaStreamWaitEvent(st, p->done, 0));
+  return GFFT_OK;
+}
+
+gfft_status mark_call_done(gfft_plan_uneven* p, cudaStream_t st) {
+  if (capturing(st)) return GFFT_OK;
+  GFFT_CUDA(cudaEventRecord(p->done, st));
+  return GFFT_OK;
+}
+}  // namespace
 
 extern "C" GFFT_API void gfft_plan_uneven_close(gfft_plan_uneven* p);
 
@@ -265,6 +294,7 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
   }
   GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
   GFFT_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+  GFFT_CUDA(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
   return GFFT_OK;
 }
 
@@ -360,7 +390,9 @@ gfft_status gfft_plan_uneven_new(gfft_plan_uneven** out, int32_t precision, int6
   if (opts) o = *opts;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GFFT_ERR_NO_DEVICE;
-  GFFT_CUDA(cudaSetDevice(o.device));
+  if (o.device < 0 || o.device >= ndev) return GFFT_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(o.device));
   auto* p = new (std::nothrow) gfft_plan_uneven;
   if (!p) return GFFT_ERR_OUT_OF_MEMORY;
   p->prec = precision;
@@ -402,6 +434,7 @@ void gfft_plan_uneven_close(gfft_plan_uneven* p) {
   if (p->tab) cudaFree(p->tab);
   if (p->counters) cudaFree(p->counters);
   if (p->cap) cudaStreamDestroy(p->cap);
+  if (p->done) cudaEventDestroy(p->done);
   delete p;
 }
 
@@ -415,10 +448,30 @@ gfft_status gfft_uneven_exec(gfft_plan_uneven* p, int32_t direction, void* dst, 
   if (direction != -1 && direction != 1) return GFFT_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> g(p->mu);  // the plan's work buffers are shared
-  if (!use_graph) return uneven_dispatch(p, direction, dst, src, st);
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->device));
+  gfft_status s0 = after_previous_call(p, st);
+  if (s0 != GFFT_OK) return s0;
+  if (!use_graph) {
+    s0 = uneven_dispatch(p, direction, dst, src, st);
+    return s0 != GFFT_OK ? s0 : mark_call_done(p, st);
+  }
   cudaGraphExec_t exec = nullptr;
+  ++p->tick;
   for (auto& gr : p->graphs)
-    if (gr.dir == direction && gr.src == src && gr.dst == dst) exec = gr.exec;
+    if (gr.dir == direction && gr.src == src && gr.dst == dst) {
+      exec = gr.exec;
+      gr.used = p->tick;
+    }
+  if (!exec && p->graphs.size() >= kMaxGraphs) {
+    // drop the least recently used graph; every replay of it has finished
+    // once the plan's previous call has (calls are ordered on the device)
+    auto lru = std::min_element(p->graphs.begin(), p->graphs.end(),
+                                [](const auto& a, const auto& b) { return a.used < b.used; });
+    GFFT_CUDA(cudaEventSynchronize(p->done));
+    cudaGraphExecDestroy(lru->exec);
+    p->graphs.erase(lru);
+  }
   if (!exec) {
     cudaGraph_t graph = nullptr;
     GFFT_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
@@ -432,10 +485,10 @@ gfft_status gfft_uneven_exec(gfft_plan_uneven* p, int32_t direction, void* dst, 
     e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
-    p->graphs.push_back({direction, src, dst, exec});
+    p->graphs.push_back({direction, src, dst, exec, p->tick});
   }
   GFFT_CUDA(cudaGraphLaunch(exec, st));
-  return GFFT_OK;
+  return mark_call_done(p, st);
 }
 
 gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* p, int32_t direction, void* dst, const void* src,
@@ -446,6 +499,10 @@ gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* p, int32_t direction, vo
   if (direction != -1 && direction != 1) return GFFT_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::lock_guard<std::mutex> g(p->mu);
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(p->device));
+  gfft_status s0 = after_previous_call(p, st);
+  if (s0 != GFFT_OK) return s0;
   const size_t es = elem_bytes(p->prec);
   for (int64_t i = 0; i < p->count; ++i) {
     const int64_t n = p->len[i];
@@ -465,7 +522,7 @@ gfft_status gfft_uneven_exec_per_size(gfft_plan_uneven* p, int32_t direction, vo
                               static_cast<const char*>(src) + size_t(p->off[i]) * es, 1, n, n, st);
     if (s != GFFT_OK) return s;
   }
-  return GFFT_OK;
+  return mark_call_done(p, st);
 }
 
 }  // extern "C"

@@ -42,9 +42,9 @@ SWEEP = [2 ** k for k in range(4, 25)]
 WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^4..2^24, 1 GiB batch per N"
 
 # DRAM bytes per transform (read + write, all passes) of the multi-pass
-# plans, from ncu captures of small batches (profiles/k_tp_split_n16777216.md,
-# profiles/k_tp3_n8388608.md, profiles/k_tp3t_n8388608.md); used to scale
-# `roofline.traffic` to a launch.
+# plans, each the sum of dram__bytes_read.sum and dram__bytes_write.sum over
+# the passes of one ncu capture of a 16-transform batch of that plan, divided
+# by 16; used to scale `roofline.traffic` to a launch.
 TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6,
                          "gpu-sm100-tp3-256x256x128": 359.4e6,
                          "gpu-sm100-tp3t-256x256x128-t4096-e16-s3": 363.4e6}
@@ -304,7 +304,7 @@ def _median_ms(fn, stream, iters: int, warm: int = 1) -> float:
     return statistics.median(ts)
 
 
-EXTRAS = ("c128_sweep", "real", "uneven", "mixed_radix", "bluestein", "precision_form", "convolve")
+EXTRAS = ("config1", "c128_sweep", "real", "uneven", "mixed_radix", "bluestein", "precision_form", "convolve")
 
 
 def extras(dev, stream, iters: int, only=EXTRAS) -> dict:
@@ -316,6 +316,8 @@ def extras(dev, stream, iters: int, only=EXTRAS) -> dict:
     out = {}
     gen = torch.Generator(device=dev)
     gen.manual_seed(77)
+    if "config1" in only:
+        out.update(_config1(dev, stream, iters))
     if "c128_sweep" in only:
         out.update(_c128_sweep(dev, stream, iters, gen))
     if "real" in only:
@@ -331,6 +333,86 @@ def extras(dev, stream, iters: int, only=EXTRAS) -> dict:
     if "convolve" in only:
         out.update(_convolve(dev, stream, iters, gen))
     return out
+
+
+def _flush_l2(buf):
+    """Overwrites a buffer larger than the 126 MB L2."""
+    buf.add_(1.0)
+
+
+def _config1(dev, stream, iters):
+    """The reference's CPU-runnable batch: complex64 N = 1024, count = 256,
+    Re/Im i.i.d. U[-1, 1) float32 from seed 0, ForwardBatch then
+    InverseBatch.  Device time per forward+inverse pair (L2 flushed before
+    each pair: the 2 MiB batch would otherwise stay in L2), end-to-end time
+    through the host-slice API from pageable numpy arrays (as Go slices
+    arrive), and the errors of both results against the oracle's
+    restatement of the reference path and the FP64 naive DFT."""
+    import numpy as np
+    import torch
+    import algofft
+    import oracle
+    n, count = 1024, 256
+    rng = np.random.default_rng(0)
+    re = rng.uniform(-1.0, 1.0, n * count).astype(np.float32)
+    im = rng.uniform(-1.0, 1.0, n * count).astype(np.float32)
+    x = (re + 1j * im).astype(np.complex64)
+    src = torch.from_numpy(x).to(dev)
+    fwd = torch.empty_like(src)
+    back = torch.empty_like(src)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    ts = []
+    with algofft.NewPlan(n) as p:
+        for it in range(iters + 3):
+            _flush_l2(flush)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            p.ForwardBatch(fwd, src, count)
+            p.InverseBatch(back, fwd, count)
+            b.record(stream)
+            b.synchronize()
+            if it >= 3:
+                ts.append(a.elapsed_time(b))
+        hf = np.empty_like(x)
+        hb = np.empty_like(x)
+        for _ in range(3):
+            p.ForwardBatch(hf, x, count)
+            p.InverseBatch(hb, hf, count)
+        e2e = []
+        for _ in range(max(5, iters)):
+            t0 = time.perf_counter()
+            p.ForwardBatch(hf, x, count)
+            p.InverseBatch(hb, hf, count)
+            e2e.append(time.perf_counter() - t0)
+        torch.cuda.synchronize()
+        f = fwd.cpu().numpy()
+        bk = back.cpu().numpy()
+    ms = statistics.median(ts)
+    byts = 2 * 16 * n * count  # forward and inverse, one read and one write each
+
+    def errs(got, want):
+        got = got.astype(np.complex128)
+        want = want.astype(np.complex128)
+        return {"rel_l2": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+                "max_err_rel_to_max": float(np.max(np.abs(got - want)) / np.max(np.abs(want)))}
+
+    rows = x.reshape(count, n)
+    exact_f = np.concatenate([oracle.naive_dft(r) for r in rows])
+    exact_b = np.concatenate([oracle.naive_dft(r, True) for r in f.reshape(count, n)])
+    return {"config1_c64_1024x256_fwd_inv": {
+        "unit": "GB/s", "bytes_per_pair": byts, "device_ms_per_pair": ms,
+        "device_gbs": byts / (ms / 1e3) / 1e9, "transforms_per_s": 2 * count / (ms / 1e3),
+        "l2": "flushed (256 MB written) before each timed pair",
+        "e2e_ms_per_pair": statistics.median(e2e) * 1e3,
+        "e2e_gbs": byts / statistics.median(e2e) / 1e9,
+        "e2e_path": "host-slice API from pageable numpy arrays, copies inside the call",
+        "forward_vs_oracle_restatement": errs(f, oracle.batch(x, n)),
+        "forward_vs_fp64_dft": errs(f, exact_f),
+        "inverse_vs_oracle_restatement": errs(bk, oracle.batch(f, n, inverse=True)),
+        "inverse_vs_fp64_dft": errs(bk, exact_b),
+        "round_trip_rel_l2": errs(bk, x)["rel_l2"],
+        "tolerance": "rel L2 <= 1e-6*log2(N) = 1e-5"}}
 
 
 def _c128_sweep(dev, stream, iters, gen):
@@ -382,7 +464,13 @@ def _real(dev, stream, iters, gen):
 
 
 def _uneven(dev, stream, iters, gen):
-    """Uneven-length batch: one plan, graph replay, against the per-size path."""
+    """Uneven-length batch: one plan, graph replay, against the plain
+    per-size GPU path -- one ForwardBatch per distinct length over that
+    length's transforms held contiguously (the data grouped by length ahead
+    of time, so the baseline pays no gather) -- and, labelled separately,
+    against one Forward call per transform.  Accuracy: every transform of
+    the uneven plan against the per-length batches, and the first 40 against
+    numpy's FP64 FFT."""
     import numpy as np
     import torch
     import algofft
@@ -396,19 +484,56 @@ def _uneven(dev, stream, iters, gen):
         ps_ms = _median_ms(lambda: p.ForwardPerSize(yu, xu), stream, 2)
         p.Forward(yu, xu)
         torch.cuda.synchronize()
+        # the same data grouped by length: one contiguous batch per length
+        offs = np.concatenate([[0], np.cumsum(L)[:-1]])
+        order = np.argsort(L, kind="stable")
+        idx = np.concatenate([np.arange(offs[i], offs[i] + L[i]) for i in order])
+        idx_t = torch.from_numpy(idx).to(dev)
+        xg = xu.index_select(0, idx_t)
+        yg = torch.empty_like(xg)
+        lens, counts = np.unique(L, return_counts=True)
+        t0 = time.perf_counter()
+        plans = [algofft.NewPlan(int(n)) for n in lens]
+        plan_s = time.perf_counter() - t0
+        views, at = [], 0
+        for n, c in zip(lens, counts):
+            m = int(n) * int(c)
+            views.append((xg[at:at + m], yg[at:at + m], int(c)))
+            at += m
+
+        def per_length():
+            for pl, (xv, yv, c) in zip(plans, views):
+                pl.ForwardBatch(yv, xv, c)
+
+        pl_ms = _median_ms(per_length, stream, 3)
+        per_length()
+        torch.cuda.synchronize()
+        y_grouped = yu.index_select(0, idx_t)
+        diff = float(torch.linalg.vector_norm(y_grouped - yg) / torch.linalg.vector_norm(yg))
+        for pl in plans:
+            pl.Close()
         xh = xu[:int(L[:40].sum())].cpu().numpy().astype(np.complex128)
         yh = yu[:int(L[:40].sum())].cpu().numpy()
+        del xg, yg, idx_t, y_grouped
     errs, off = [], 0
     for n in L[:40]:
         r = np.fft.fft(xh[off:off + n])
         errs.append(float(np.linalg.norm(yh[off:off + n] - r) / np.linalg.norm(r)))
         off += n
-    out["uneven_20000"] = {"transforms": 20000, "elements": int(tot),
-                           "transforms_per_s": 20000 / (g_ms / 1e3),
-                           "per_size_transforms_per_s": 20000 / (ps_ms / 1e3),
-                           "speedup_vs_per_size": ps_ms / g_ms, "ms": g_ms, "per_size_ms": ps_ms,
+    out["uneven_20000"] = {"transforms": 20000, "elements": int(tot), "distinct_lengths": int(lens.size),
+                           "ms": g_ms, "transforms_per_s": 20000 / (g_ms / 1e3),
                            "gbs_user_bytes": 16 * tot / (g_ms / 1e3) / 1e9,
-                           "max_rel_l2_first_40": max(errs)}
+                           "per_length_batched_ms": pl_ms,
+                           "per_length_batched_transforms_per_s": 20000 / (pl_ms / 1e3),
+                           "speedup_vs_per_length_batched": pl_ms / g_ms,
+                           "per_length_plan_creation_s": plan_s,
+                           "per_transform_loop_ms": ps_ms,
+                           "speedup_vs_per_transform_loop": ps_ms / g_ms,
+                           "baselines": "per_length_batched: one ForwardBatch per distinct length over that "
+                                        "length's transforms grouped contiguously (no gather timed); "
+                                        "per_transform_loop: one Forward per transform (gfft_uneven_exec_per_size)",
+                           "rel_l2_all_vs_per_length_batched": diff,
+                           "max_rel_l2_first_40_vs_fp64": max(errs)}
     del xu, yu
     return out
 
@@ -641,17 +766,17 @@ def main():
         ref = oracle.batch(xs, n)
         errs[n] = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
-    # end to end: the same sweep through the host-slice API (pinned host
-    # buffers; copies in, transforms and copies out inside the timed region,
-    # every step), timed on the host around whole calls
+    # end to end: the same sweep through the host-slice API, copies in,
+    # transforms and copies out inside the timed region every step, timed on
+    # the host around whole calls.  The headline uses pageable numpy arrays,
+    # as Go slices arrive (the library stages them through its pinned
+    # lanes); the same sweep from pinned buffers is reported beside it.
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
-    e2e_val = None
-    if e2e_steps:
-        hx_t = torch.empty(xin.numel(), dtype=torch.complex64, pin_memory=True)
-        hx_t.copy_(xin)
-        hy_t = torch.empty_like(hx_t, pin_memory=True)
-        host = {n: (hx_t.numpy(), hy_t.numpy(), bufs[n][2]) for n in SWEEP}
-        for n in SWEEP:  # warm the staging pool
+    e2e_val = e2e_pinned = None
+
+    def host_sweep(hx_all, hy_all):
+        host = {n: (hx_all, hy_all, bufs[n][2]) for n in SWEEP}
+        for n in SWEEP:  # warm the staging pools
             hx, hy, count = host[n]
             plans[n].ForwardBatch(hy, hx, count)
         if pg:
@@ -662,8 +787,19 @@ def main():
                 hx, hy, count = host[n]
                 plans[n].ForwardBatch(hy, hx, count)
         e2e_s = max_over_ranks(time.perf_counter() - t0, pg, dev)
-        e2e_val = world * bytes_step * e2e_steps / max(e2e_s, 1e-9) / 1e9
-        del hx_t, hy_t, host
+        return world * bytes_step * e2e_steps / max(e2e_s, 1e-9) / 1e9
+
+    if e2e_steps:
+        hx_np = xin.cpu().numpy()          # pageable
+        hy_np = np.empty_like(hx_np)
+        hy_np.fill(0)                      # fault the pages in before timing
+        e2e_val = host_sweep(hx_np, hy_np)
+        del hy_np
+        hx_t = torch.empty(xin.numel(), dtype=torch.complex64, pin_memory=True)
+        hx_t.copy_(xin)
+        hy_t = torch.empty_like(hx_t, pin_memory=True)
+        e2e_pinned = host_sweep(hx_t.numpy(), hy_t.numpy())
+        del hx_t, hy_t, hx_np
 
     ext = None
     if rank == 0 and not args.no_extras and world == 1:
@@ -692,8 +828,11 @@ def main():
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": "GB/s", "h2d_bytes_per_step": bytes_step // 2,
                     "d2h_bytes_per_step": bytes_step // 2, "steps": e2e_steps,
-                    "path": "Plan.ForwardBatch on pinned host slices (gfft_forward_batch_host: 64 MB chunks, "
-                            "copy in / transform / copy out pipelined over two streams)"},
+                    "path": "Plan.ForwardBatch on pageable host slices (gfft_forward_batch_host: 32 MB chunks "
+                            "staged through three library-owned pinned lanes, host copies by a thread pool "
+                            "overlapped with the lanes' device copies and transforms)",
+                    "pinned_value": e2e_pinned,
+                    "pinned_path": "the same sweep from pinned host buffers (64 MB chunks, no host copies)"},
             "gpu_launches": args.steps * launches_step,
         }
         if ext is not None:

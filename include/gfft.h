@@ -3,9 +3,13 @@
  * batched-transform path.
  *
  * Every entry point takes plain pointers and sizes and returns a status code,
- * so a cgo binding can call it directly.  Each entry
- * point names the reference API it replaces as file:line inside
- * CWBudde/algo-fft.
+ * so a cgo binding can call it directly.  Each entry point names the
+ * reference API it replaces as file:line inside CWBudde/algo-fft.
+ *
+ * Devices: a plan lives on the device of its options; every call on it runs
+ * with that device current and gives the calling thread its previous current
+ * device back before returning.  A stream passed in must belong to the
+ * plan's device (or be NULL).
  *
  * Conventions
  *  - Complex data is interleaved (re, im): complex64 = 2 x float32,
@@ -199,7 +203,12 @@ GFFT_API gfft_status gfft_inverse_strided(gfft_plan* plan, void* dst, int64_t ds
  * bytes of it at most 63.5 MiB (n <= 2^21 complex64, 2^20 complex128);
  * larger lengths, or plans on another schedule, are rejected with an error.
  * The first call on a device looks the array up (make it before any stream
- * capture).  All calls share the array: calls that overlap on the GPU race. */
+ * capture).  All calls share the array: calls that overlap on the GPU race.
+ * The kernel's waits are bounded: if one expires, that call stops early and
+ * leaves dst incomplete, and the plan's status word is set, which
+ * gfft_plan_check then reports as GFFT_ERR_TIMEOUT (the next call starts
+ * afresh).  A caller that must know a call completed checks the plan after
+ * synchronizing its stream. */
 GFFT_API gfft_status gfft_exec_batch_noalloc(gfft_plan* plan, int32_t direction, void* dst, int64_t dst_len,
                                              const void* src, int64_t src_len, int64_t count, void* stream);
 
@@ -336,8 +345,13 @@ GFFT_API int64_t gfft_plan_uneven_total(const gfft_plan_uneven* plan);
 /* The whole batch in a few launches (persistent work-queue kernel for
  * every transform that fits one CTA, grouped batches for the rest),
  * replayed from a CUDA graph captured on first use per (direction, dst,
- * src) when use_graph is set.  dst may equal src.  Calls on one plan are
- * serialized (they share its work buffers). */
+ * src) when use_graph is set (the plan keeps the 8 most recently used
+ * graphs).  dst may equal src.  Safe to call from several threads and
+ * streams at once: the calls of one plan share its work buffers, so each is
+ * ordered on the device after the plan's previous call (an event recorded
+ * by every call, waited on by the next; the calls do not overlap on the
+ * GPU).  Inside a caller's own stream capture that ordering is left to the
+ * captured graph. */
 GFFT_API gfft_status gfft_uneven_exec(gfft_plan_uneven* plan, int32_t direction, void* dst, const void* src,
                                       int32_t use_graph, void* stream);
 /* The plain per-size path: one plan per distinct length and one transform

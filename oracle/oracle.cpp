@@ -522,6 +522,76 @@ void orc_naive_dft_ref(const double* in, double* out, int64_t n, int inverse) {
   }
 }
 
+// internal/reference/dft2d.go:17-160 NaiveDFT2D / NaiveIDFT2D (and the
+// complex128 forms) and internal/reference/dft3d.go:18-146 NaiveDFT3D /
+// NaiveIDFT3D, generalised over the axis count: row-major input
+// x[i0*d1*..*d(r-1) + ...], output bin (k0, .., k(r-1)) in the same order;
+// per input sample the phase is the sum over axes of ∓2π·k_a·m_a/d_a, each
+// term formed in float64 without reduction exactly as the reference does,
+// then cos/sin of the sum, complex128 accumulation, the inverse scaled by
+// 1/(d0·..·d(r-1)).  The complex64 reference versions round the complex128
+// sum to complex64 at the end; the caller does that cast.
+void orc_naive_dft_nd_ref(const double* in, double* out, int ndims, const int64_t* dims, int inverse) {
+  const auto* x = reinterpret_cast<const cx<double>*>(in);
+  auto* y = reinterpret_cast<cx<double>*>(out);
+  int64_t total = 1;
+  for (int a = 0; a < ndims; ++a) total *= dims[a];
+  const double sgn = inverse ? 2.0 : -2.0;
+  std::vector<int64_t> k(ndims), m(ndims);
+  for (int64_t kk = 0; kk < total; ++kk) {
+    for (int64_t r = kk, a = ndims - 1; a >= 0; --a) {
+      k[a] = r % dims[a];
+      r /= dims[a];
+    }
+    cx<double> s{0, 0};
+    for (int64_t mm = 0; mm < total; ++mm) {
+      for (int64_t r = mm, a = ndims - 1; a >= 0; --a) {
+        m[a] = r % dims[a];
+        r /= dims[a];
+      }
+      double phase = 0;
+      for (int a = 0; a < ndims; ++a) phase += sgn * kPi * double(k[a] * m[a]) / double(dims[a]);
+      s = s + x[mm] * cx<double>{std::cos(phase), std::sin(phase)};
+    }
+    if (inverse) s = s * cx<double>{1.0 / double(total), 0};
+    y[kk] = s;
+  }
+}
+
+// FP64 N-D arbiter: the same sum with every axis term reduced exactly
+// (k_a·m_a mod d_a in integers) and the phase accumulated as a fraction of
+// a turn in long double, long double accumulation of the products.
+void orc_naive_dft_nd_f64(const double* in, double* out, int ndims, const int64_t* dims, int inverse) {
+  const auto* x = reinterpret_cast<const cx<double>*>(in);
+  auto* y = reinterpret_cast<cx<double>*>(out);
+  int64_t total = 1;
+  for (int a = 0; a < ndims; ++a) total *= dims[a];
+  const long double sgn = inverse ? 1.0L : -1.0L;
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  std::vector<int64_t> k(ndims), m(ndims);
+  for (int64_t kk = 0; kk < total; ++kk) {
+    for (int64_t r = kk, a = ndims - 1; a >= 0; --a) {
+      k[a] = r % dims[a];
+      r /= dims[a];
+    }
+    long double sr = 0, si = 0;
+    for (int64_t mm = 0; mm < total; ++mm) {
+      for (int64_t r = mm, a = ndims - 1; a >= 0; --a) {
+        m[a] = r % dims[a];
+        r /= dims[a];
+      }
+      long double turn = 0;
+      for (int a = 0; a < ndims; ++a) turn += (long double)((k[a] * m[a]) % dims[a]) / (long double)dims[a];
+      turn -= std::floor(turn);
+      const long double c = std::cos(sgn * two_pi * turn), sn = std::sin(sgn * two_pi * turn);
+      sr += (long double)x[mm].re * c - (long double)x[mm].im * sn;
+      si += (long double)x[mm].re * sn + (long double)x[mm].im * c;
+    }
+    const long double s = inverse ? 1.0L / (long double)total : 1.0L;
+    y[kk] = {double(sr * s), double(si * s)};
+  }
+}
+
 // The reference's algorithm choice for n (plan.go:343-368): 0 DIT,
 // 1 Stockham, 2 six-step, 3 mixed radix, 4 Bluestein.
 int orc_algorithm(int64_t n) { return choose(n); }

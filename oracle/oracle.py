@@ -40,6 +40,8 @@ def lib():
         I = ctypes.c_int
         L.orc_naive_dft_f64.argtypes = [P, P, I64, I]
         L.orc_naive_dft_ref.argtypes = [P, P, I64, I]
+        L.orc_naive_dft_nd_ref.argtypes = [P, P, I, P, I]
+        L.orc_naive_dft_nd_f64.argtypes = [P, P, I, P, I]
         L.orc_algorithm.argtypes = [I64]
         L.orc_batch_c64.argtypes = [P, P, I64, I64, I, I]
         L.orc_batch_c128.argtypes = [P, P, I64, I64, I, I]
@@ -79,6 +81,27 @@ def naive_dft_ref(x: np.ndarray, inverse: bool = False) -> np.ndarray:
     y = np.empty_like(x)
     lib().orc_naive_dft_ref(_p(x), _p(y), x.size, int(inverse))
     return y
+
+
+def _nd(fn, x: np.ndarray, dims, inverse: bool) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.complex128).ravel()
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.int64))
+    if int(np.prod(d)) != x.size:
+        raise ValueError("input length must equal the product of the dimensions")
+    y = np.empty_like(x)
+    fn(_p(x), _p(y), int(d.size), _p(d), int(inverse))
+    return y
+
+
+def naive_dft_nd(x: np.ndarray, dims, inverse: bool = False) -> np.ndarray:
+    """FP64 N-D arbiter (exact per-axis angle reduction), row-major."""
+    return _nd(lib().orc_naive_dft_nd_f64, x, dims, inverse)
+
+
+def naive_dft_nd_ref(x: np.ndarray, dims, inverse: bool = False) -> np.ndarray:
+    """The reference's NaiveDFT2D/3D formula (internal/reference/dft2d.go,
+    dft3d.go), complex128 result (the complex64 versions round it)."""
+    return _nd(lib().orc_naive_dft_nd_ref, x, dims, inverse)
 
 
 def algorithm(n: int) -> int:

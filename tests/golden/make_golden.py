@@ -108,3 +108,73 @@ cases.append({"name": "convolve_real_basic", "cite": "convolve_real_test.go:10",
 with open(os.path.join(HERE, "known_answers.json"), "w") as f:
     json.dump({"generator": "tests/golden/make_golden.py", "cases": cases}, f, indent=0)
 print(f"wrote {len(cases)} cases")
+
+
+# ---- N-D cases (plan_2d_test.go:202-383, plan_3d_test.go:237-380) ----------
+# The reference builds its inputs with Go's PCG generator
+# (generateRandom2DSignal, plan_2d_test.go:15-26: re and im each
+# rng.Float64()*20 - 10, cast to float32).  Go's stream is not reproduced
+# here; the fixtures keep the tests' shapes, value distribution (U[-10, 10)
+# float32), batch/stride layouts and tolerances, with inputs from numpy's
+# seeded generator and expected values from the exact N-D DFT (axis by axis
+# in 50-digit arithmetic), i.e. what NaiveDFT2D / NaiveDFT3D approximate.
+import numpy as np  # noqa: E402
+
+
+def exact_dft_nd(x, dims, inverse=False):
+    a = np.empty(dims, dtype=object)
+    flat = a.reshape(-1)
+    for i, v in enumerate(x):
+        flat[i] = mpmath.mpc(v[0], v[1])
+    for ax, n in enumerate(dims):
+        a = np.moveaxis(a, ax, -1)
+        out = np.empty_like(a)
+        sgn = 1 if inverse else -1
+        w = [mpmath.expjpi(mpmath.mpf(sgn * 2 * j) / n) for j in range(n)]
+        for idx in np.ndindex(*a.shape[:-1]):
+            row = a[idx]
+            for k in range(n):
+                s = mpmath.mpc(0)
+                for j in range(n):
+                    s += row[j] * w[(j * k) % n]
+                out[idx + (k,)] = s / n if inverse else s
+        a = np.moveaxis(out, -1, ax)
+    return [[float(v.real), float(v.imag)] for v in a.reshape(-1)]
+
+
+def nd_input(dims, seed, prec):
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(dims))
+    re = rng.random(n) * 20 - 10
+    im = rng.random(n) * 20 - 10
+    if prec == "complex64":
+        re, im = re.astype(np.float32).astype(np.float64), im.astype(np.float32).astype(np.float64)
+    return [[float(a), float(b)] for a, b in zip(re, im)]
+
+
+nd_cases = []
+for dims, kind, prec, tol, cite in (
+        [((r, c), "forward", "complex64", 1e-3, "plan_2d_test.go:202") for r, c in
+         ((2, 2), (4, 4), (8, 8), (16, 16), (4, 8), (8, 4))] +
+        [((r, c), "inverse", "complex64", 1e-3, "plan_2d_test.go:250") for r, c in
+         ((2, 2), (4, 4), (8, 8), (16, 16), (4, 8))] +
+        [((r, c), "forward", "complex128", 1e-10, "plan_2d_test.go:339") for r, c in ((4, 4), (8, 8), (4, 8))] +
+        [(d, "forward", "complex64", 1e-2, "plan_3d_test.go:237") for d in
+         ((2, 2, 2), (4, 4, 4), (8, 8, 8), (4, 8, 16))] +
+        [(d, "forward", "complex128", 1e-9, "plan_3d_test.go:339") for d in ((2, 2, 2), (4, 4, 4), (8, 8, 8))]):
+    seed = int(np.prod(dims)) * 7 + len(dims) + (1 if kind == "inverse" else 0) + (2 if prec == "complex128" else 0)
+    x = nd_input(dims, seed, prec)
+    nd_cases.append({"name": f"{'x'.join(map(str, dims))}_{kind}_{prec}", "cite": cite, "dims": list(dims),
+                     "kind": kind, "precision": prec, "input": x, "expected": exact_dft_nd(x, dims, kind == "inverse"),
+                     "tol_abs": tol})
+
+# batch + stride layouts: plan_2d_test.go:294-337 (4x4, batch 2, stride 21)
+# and plan_3d_test.go:293-330 (2x3x4, batch 2, stride 31), tolerance 1e-3.
+for dims, stride, cite in (((4, 4), 21, "plan_2d_test.go:294"), ((2, 3, 4), 31, "plan_3d_test.go:293")):
+    sig = [nd_input(dims, 100 + b, "complex64") for b in range(2)]
+    nd_cases.append({"name": f"{'x'.join(map(str, dims))}_batch2_stride{stride}", "cite": cite, "dims": list(dims),
+                     "kind": "forward_batch", "precision": "complex64", "batch": 2, "stride": stride,
+                     "input": sig, "expected": [exact_dft_nd(s, dims) for s in sig], "tol_abs": 1e-3})
+
+with open(os.path.join(HERE, "nd_known_answers.json"), "w") as f:
+    json.dump({"generator": "tests/golden/make_golden.py", "cases": nd_cases}, f, indent=0)

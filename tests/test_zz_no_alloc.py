@@ -60,3 +60,27 @@ def test_noalloc_rejects_what_it_cannot_hold():
     with algofft.NewPlan(1024) as p:  # single-pass schedule: not this kernel
         a = torch.zeros(1024, dtype=torch.complex64, device="cuda")
         assert _noalloc(p, -1, a, a, 1) == algofft.ErrNotImplemented.status
+
+
+@pytest.mark.parametrize("n,count", [(1 << 16, 17), (1 << 16, 3), (1 << 15, 33)])
+def test_noalloc_partial_last_group(n, count):
+    """Batches that end in a partial group of transforms (the plan groups 16
+    transforms of 2^16 points and 32 of 2^15 per scratch slot): the entry
+    point against the regular one and against numpy's FP64 FFT, two calls in
+    a row."""
+    import torch
+    tok = next(t for t in algofft.Variants(n) if "-tp-" in t)
+    with algofft.Plan(n, variant=tok) as p:
+        for call in range(2):
+            x = seeded_complex(n * count, seed=200 + call)
+            src = torch.from_numpy(x).cuda()
+            want = torch.empty_like(src)
+            got = torch.full_like(src, float("nan"))
+            p.ForwardBatch(want, src, count)
+            assert _noalloc(p, -1, got, src, count) == 0, algofft.lib().gfft_last_error()
+            torch.cuda.synchronize()
+            p.Check()
+            g = got.cpu().numpy()
+            assert rel_l2(g, want.cpu().numpy()) <= tol_c2c(n, False)
+            ref = np.fft.fft(x.astype(np.complex128).reshape(count, n), axis=1)
+            assert rel_l2(g.reshape(count, n), ref) <= tol_c2c(n, False)
