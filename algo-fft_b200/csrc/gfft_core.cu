@@ -8,6 +8,7 @@
 #include <vector>
 #include "gfft_internal.h"
 #include "gfft_math.cuh"
+#include "gfft_l2pipe.cuh"
 #include "gfft_threepass.cuh"
 #include "gfft_twopass.cuh"
 
@@ -48,6 +49,28 @@ std::vector<const ThreePassKernel*> threepass_variants(int prec, int64_t n, int 
   return v;
 }
 void register_twopass(const TwoPassKernel& k) { twopass_table().push_back(k); }
+
+static std::vector<L2PipeKernel>& l2pipe_table() {
+  static std::vector<L2PipeKernel> t;
+  return t;
+}
+
+void register_l2pipe(const L2PipeKernel& k) { l2pipe_table().push_back(k); }
+
+const L2PipeKernel* find_l2pipe(int prec, int64_t n, int dir, int n1, int nc1, int nc2, int nst) {
+  for (const auto& k : l2pipe_table())
+    if (k.prec == prec && int64_t(k.n1) * k.n2 == n && k.dir == dir && (n1 == 0 || k.n1 == n1) &&
+        (nc1 == 0 || k.nc1 == nc1) && (nc2 == 0 || k.nc2 == nc2) && (nst == 0 || k.nst == nst))
+      return &k;
+  return nullptr;
+}
+
+std::vector<const L2PipeKernel*> l2pipe_variants(int prec, int64_t n, int dir) {
+  std::vector<const L2PipeKernel*> v;
+  for (const auto& k : l2pipe_table())
+    if (k.prec == prec && int64_t(k.n1) * k.n2 == n && k.dir == dir) v.push_back(&k);
+  return v;
+}
 
 const TwoPassKernel* find_twopass(int prec, int64_t n, int dir, int te, int emax) {
   for (const auto& k : twopass_table())
@@ -258,6 +281,37 @@ static gfft_status init_twopass(PlanCore* c, const TwoPassKernel* f, const TwoPa
   return GFFT_OK;
 }
 
+static std::string l2pipe_token(const L2PipeKernel* k, int gmb) {
+  return "gpu-sm100-l2p-" + std::to_string(k->n1) + "x" + std::to_string(k->n2) + "-c" + std::to_string(k->nc1) +
+         "x" + std::to_string(k->nc2) + "-e" + std::to_string(k->ept1) + "x" + std::to_string(k->ept2) + "-s" +
+         std::to_string(k->nst) + "-g" + std::to_string(gmb);
+}
+
+// L2-pipelined plan: the two-pass tables of the same split (and its split
+// kernels, for buffers the copy engine cannot address), groups of about
+// gmb MB in three scratch slots.
+static gfft_status init_l2pipe(PlanCore* c, const L2PipeKernel* f, const L2PipeKernel* inv, int gmb) {
+  const TwoPassKernel* tf = nullptr;
+  const TwoPassKernel* ti = nullptr;
+  for (const TwoPassKernel* k : twopass_variants(c->prec, c->n, -1))
+    if (k->n1 == f->n1 && !tf) tf = k;
+  for (const TwoPassKernel* k : twopass_variants(c->prec, c->n, +1))
+    if (k->n1 == f->n1 && tf && k->te == tf->te && k->emax == tf->emax) ti = k;
+  if (!tf || !ti) {
+    set_error("no two-pass kernel of the split " + std::to_string(f->n1) + " x " + std::to_string(f->n2));
+    return GFFT_ERR_NOT_IMPLEMENTED;
+  }
+  gfft_status s = init_twopass(c, tf, ti);
+  if (s != GFFT_OK) return s;
+  c->l2[0] = f;
+  c->l2[1] = inv;
+  c->l2_gmb = gmb;
+  c->l2_slots = 3;
+  c->algo = Algo::L2Pipe;
+  c->name = l2pipe_token(f, gmb);
+  return GFFT_OK;
+}
+
 // Three-pass plan: W_N1 | W_M1 | W_M2 | split W_N | split W_M in one
 // allocation.
 static gfft_status init_threepass(PlanCore* c, const ThreePassKernel* f, const ThreePassKernel* inv) {
@@ -317,6 +371,8 @@ std::vector<std::string> variant_tokens(int prec, int64_t n) {
     if (n <= (prec == kC64 ? 16384 : 8192))
       for (const Pow2Kernel* k : pow2_variants(prec, int(n), -1)) v.push_back(pow2_token(k->n, k->ept));
     for (const TwoPassKernel* k : twopass_variants(prec, n, -1)) v.push_back(twopass_token(k));
+    for (const L2PipeKernel* k : l2pipe_variants(prec, n, -1))
+      for (int gmb : {8, 16}) v.push_back(l2pipe_token(k, gmb));
     for (const ThreePassKernel* k : threepass_variants(prec, n, -1)) v.push_back(threepass_token(k));
   } else if (n > 1 && is_smooth7(n)) {
     // runtime-radix schedules (single CTA when it fits, two passes when n
@@ -363,6 +419,16 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     if (f && i && f->n1 == a && f->m1 == b && f->m2 == te) return init_threepass(c, f, i);
   }
   int m2 = 0, ns = 0;
+  {
+    int c1 = 0, c2 = 0, e1 = 0, e2 = 0, gmb = 0;
+    if (std::sscanf(tok.c_str(), "gpu-sm100-l2p-%dx%d-c%dx%d-e%dx%d-s%d-g%d", &a, &b, &c1, &c2, &e1, &e2, &ns, &gmb) ==
+            8 &&
+        int64_t(a) * b == n && gmb >= 1 && gmb <= 64) {
+      const L2PipeKernel* f = find_l2pipe(prec, n, -1, a, c1, c2, ns);
+      const L2PipeKernel* i = find_l2pipe(prec, n, +1, a, c1, c2, ns);
+      if (f && i && f->ept1 == e1 && f->ept2 == e2) return init_l2pipe(c, f, i, gmb);
+    }
+  }
   if (std::sscanf(tok.c_str(), "gpu-sm100-tp3t-%dx%dx%d-t%d-e%d-s%d", &a, &b, &m2, &te, &e, &ns) == 6 &&
       int64_t(a) * b * m2 == n) {
     const ThreePassKernel* f = find_threepass(prec, n, -1, 1, te, e, ns);
@@ -575,6 +641,51 @@ static gfft_status exec_threepass(const PlanCore* c, int dir, void* dst, const v
   return GFFT_OK;
 }
 
+// L2-pipelined execution: one persistent launch over the whole batch, the
+// intermediate in S slots of G transforms (about l2_gmb MB each) that stay
+// in L2, the work counter and per-group completion counters cleared first.
+static gfft_status exec_l2pipe(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                               int64_t idist, int64_t odist, cudaStream_t st) {
+  const L2PipeKernel* k = c->l2[dir < 0 ? 0 : 1];
+  const int64_t tbytes = c->n * int64_t(elem_bytes(c->prec));
+  const int64_t G = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(c->l2_gmb) << 20) / tbytes));
+  const int64_t groups = (count + G - 1) / G;
+  const int S = c->l2_slots;
+  const int64_t tiles = groups * G * (k->n2 / k->nc1 + k->n1 / k->nc2);
+  if (tiles >= (int64_t(1) << 31)) return exec_twopass(c, dir, dst, src, count, idist, odist, st);
+  const size_t ctr_bytes = (size_t(1 + 2 * groups) * sizeof(unsigned) + 1023) & ~size_t(1023);
+  void* ws = nullptr;
+  GFFT_CUDA(ws_alloc(&ws, ctr_bytes + size_t(S) * size_t(G) * size_t(tbytes), st));
+  cudaError_t e = cudaMemsetAsync(ws, 0, ctr_bytes, st);
+  L2pParams p{};
+  p.src = src;
+  p.dst = dst;
+  p.scratch = static_cast<char*>(ws) + ctr_bytes;
+  p.ctr = static_cast<unsigned*>(ws);
+  p.status = c->status;
+  p.count = count;
+  p.idist = idist;
+  p.odist = odist;
+  p.tw1 = c->tw1;
+  p.tw2 = c->tw2;
+  p.bt.lo = c->bt_lo;
+  p.bt.hi = c->bt_hi;
+  p.bt.shift = c->bt_shift;
+  p.scale = dir < 0 ? 1.0 : 1.0 / double(c->n);
+  p.G = int(G);
+  p.S = S;
+  p.groups = int(groups);
+  p.spin_limit = 1u << 22;
+  if (e == cudaSuccess) e = k->launch(p, st);
+  cudaFreeAsync(ws, st);
+  if (e == cudaErrorNotSupported) {  // buffers the copy engine cannot address
+    cudaGetLastError();
+    return exec_twopass(c, dir, dst, src, count, idist, odist, st);
+  }
+  if (e != cudaSuccess) return cuda_status(e, "k_l2p");
+  return GFFT_OK;
+}
+
 gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
                       int64_t odist, cudaStream_t st) {
   if (count <= 0) return GFFT_OK;
@@ -593,6 +704,8 @@ gfft_status core_exec(const PlanCore* c, int dir, void* dst, const void* src, in
     }
     case Algo::TwoPass:
       return exec_twopass(c, dir, dst, src, count, idist, odist, st);
+    case Algo::L2Pipe:
+      return exec_l2pipe(c, dir, dst, src, count, idist, odist, st);
     case Algo::ThreePass:
       return exec_threepass(c, dir, dst, src, count, idist, odist, st);
     case Algo::Generic:

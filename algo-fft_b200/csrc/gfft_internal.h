@@ -45,7 +45,7 @@ class DeviceGuard {
   bool restore_ = false;
 };
 
-enum class Algo { Trivial, Pow2Smem, TwoPass, ThreePass, Generic, GenTwoPass, Bluestein, TensorCore };
+enum class Algo { Trivial, Pow2Smem, TwoPass, ThreePass, Generic, GenTwoPass, Bluestein, TensorCore, L2Pipe };
 
 // Device twiddle table W_n^m = exp(-2πi m/n), m < n, generated on the GPU in
 // FP64 and rounded to the element type (internal/math/twiddle.go:8-21).
@@ -73,6 +73,11 @@ struct PlanCore {
   const void* bt_hi = nullptr;
   int bt_shift = 0;
   int group = 1, slots = 2, resident = 1;
+  // L2-pipelined two-pass schedule (same tables as the two-pass one; tp[]
+  // holds the split kernels of the same split for buffers the copy engine
+  // cannot address): kernels, group bytes in MB and scratch slots
+  const L2PipeKernel* l2[2] = {nullptr, nullptr};
+  int l2_gmb = 16, l2_slots = 3;
   unsigned* status = nullptr;  // device word: nonzero once a bounded wait expired
   // runtime-schedule (7-smooth) plans
   GenSched gs{}, gs1{}, gs2{};

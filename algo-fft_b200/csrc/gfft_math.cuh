@@ -216,6 +216,16 @@ __device__ __forceinline__ C big_twiddle(const BigTwiddle& bt, int64_t m) {
   return w;
 }
 
+// The same from tables that may sit in shared memory (generic loads).
+template <typename C, int DIR>
+__device__ __forceinline__ C big_twiddle_any(const BigTwiddle& bt, int64_t m) {
+  const C* lo = static_cast<const C*>(bt.lo);
+  const C* hi = static_cast<const C*>(bt.hi);
+  C w = cmul(hi[m >> bt.shift], lo[m & ((int64_t(1) << bt.shift) - 1)]);
+  if constexpr (DIR > 0) w.y = -w.y;
+  return w;
+}
+
 // Streaming global accesses: the batch is touched exactly once.
 // Asks the TMA unit to bring [p, p + bytes) into L2 ahead of its use (no
 // registers, no completion to wait for).  p and bytes must be multiples of

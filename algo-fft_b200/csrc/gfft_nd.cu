@@ -485,6 +485,8 @@ gfft_status gfft_exec_strided_batch(gfft_plan* plan, int32_t direction, void* ds
   const int64_t required = (count - 1) * dist + (n - 1) * stride + 1;
   if (dst_len < required || src_len < required) return GFFT_ERR_LENGTH_MISMATCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DeviceGuard dg;
+  GFFT_CUDA(dg.set(plan->core.device));
   const int prec = plan->core.prec;
   if (stride == 1) return core_exec(&plan->core, direction, dst, src, count, dist, dist, st);
   if (dist == 1 && count <= stride) {

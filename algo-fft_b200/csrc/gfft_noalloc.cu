@@ -76,7 +76,7 @@ extern "C" gfft_status gfft_exec_batch_noalloc(gfft_plan* plan, int32_t directio
   if (count > INT64_MAX / c->n) return GFFT_ERR_LENGTH_MISMATCH;
   if (dst_len < count * c->n || src_len < count * c->n) return GFFT_ERR_LENGTH_MISMATCH;
   if (direction != -1 && direction != 1) return GFFT_ERR_INVALID_ARGUMENT;
-  if (c->algo != Algo::TwoPass) {
+  if (c->algo != Algo::TwoPass && c->algo != Algo::L2Pipe) {
     set_error("the no-allocation entry point runs the two-pass kernel only; plan '" + c->name +
               "' uses another schedule");
     return GFFT_ERR_NOT_IMPLEMENTED;

@@ -44,6 +44,21 @@ struct ThreePassKernel {
   cudaError_t (*launch)(const ThreePassParams& p, int pass, int64_t b0, int64_t nb, cudaStream_t st);
 };
 
+// L2-pipelined two-pass kernel (k_l2p) of one (precision, N1 x N2, tile
+// shape, stages, dir).
+struct L2pParams;
+struct L2PipeKernel {
+  int prec, n1, n2, nc1, nc2, ept1, ept2, nst, dir;
+  int tpb, smem;
+  const void* func;
+  cudaError_t (*launch)(const L2pParams& p, cudaStream_t st);
+};
+
+void register_l2pipe(const L2PipeKernel& k);
+// The variant of this shape and direction; nc1 = 0 takes the first registered.
+const L2PipeKernel* find_l2pipe(int prec, int64_t n, int dir, int n1 = 0, int nc1 = 0, int nc2 = 0, int nst = 0);
+std::vector<const L2PipeKernel*> l2pipe_variants(int prec, int64_t n, int dir);
+
 void register_pow2(const Pow2Kernel& k);
 void register_threepass(const ThreePassKernel& k);
 // The plain kernels (tma = 0) unless a TMA-staged variant is named.

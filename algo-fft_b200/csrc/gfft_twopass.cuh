@@ -90,12 +90,21 @@ __device__ __forceinline__ C gload(const C* p) {
   else return ld_stream(p);
 }
 
+// Barrier among the threads that run a tile's stages: the whole CTA
+// (NSYNC = 0), or the NSYNC threads of named barrier 1 (kernels whose other
+// warps copy tiles in and out and never take part in the stages).
+template <int NSYNC>
+__device__ __forceinline__ void tile_sync() {
+  if constexpr (NSYNC == 0) __syncthreads();
+  else asm volatile("bar.sync 1, %0;" ::"n"(NSYNC) : "memory");
+}
+
 // One Stockham stage of a column tile (see pow2_stage for the algebra).
 // Element (row, c) of the tile lives at sh[phys(row, c)]; global row r of
 // column c is at in[r*ISTRIDE + c].
 // ISTRIDE / OSTRIDE = 0 take the row pitch from `pitch` at run time.
 template <typename C, int L, int EPT, int NC, int DIR, int P, int LOADK, int MODE, int64_t ISTRIDE, int64_t OSTRIDE,
-          bool DENSE = false, typename IO = NoIO>
+          bool DENSE = false, typename IO = NoIO, int NSYNC = 0, bool BTG = false>
 __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
                                           int t, int c, bool active, const C* __restrict__ tw,
                                           typename RealOf<C>::type scale, const BigTwiddle& bt, int64_t n2,
@@ -123,9 +132,15 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
   [[maybe_unused]] C tw_s{}, tw_b[Q];
   if constexpr (BIGTW) {
     if (active) {
-      tw_s = big_twiddle<C, DIR>(bt, n2 * P);
+      if constexpr (BTG) {  // tables in shared memory
+        tw_s = big_twiddle_any<C, DIR>(bt, n2 * P);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) tw_b[q] = big_twiddle<C, DIR>(bt, n2 * (t + q * T));
+        for (int q = 0; q < Q; ++q) tw_b[q] = big_twiddle_any<C, DIR>(bt, n2 * (t + q * T));
+      } else {
+        tw_s = big_twiddle<C, DIR>(bt, n2 * P);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) tw_b[q] = big_twiddle<C, DIR>(bt, n2 * (t + q * T));
+      }
     }
   }
 
@@ -172,7 +187,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
         }
     }
   } else if constexpr (LAST && MODE == OUT_SMEM) {
-    if constexpr (READ_SH) __syncthreads();
+    if constexpr (READ_SH) tile_sync<NSYNC>();
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
@@ -184,7 +199,7 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
         }
     }
   } else if constexpr (LAST) {
-    if constexpr (READ_SH) __syncthreads();
+    if constexpr (READ_SH) tile_sync<NSYNC>();
     if (active) {
       C pw[RS];
       pw[0] = C{1, 0};
@@ -205,9 +220,9 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
       }
     }
     if constexpr (DENSE) fence_async_smem();  // the tile may leave by a TMA store
-    __syncthreads();
+    tile_sync<NSYNC>();
   } else {
-    if constexpr (READ_SH) __syncthreads();
+    if constexpr (READ_SH) tile_sync<NSYNC>();
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
@@ -218,8 +233,8 @@ __device__ __forceinline__ void col_stage(C* v, const C* in, C* out, C* sh,
         for (int r = 0; r < RS; ++r) sh[S::phys(j + r * P, c)] = v[q * RS + r];
       }
     }
-    __syncthreads();
-    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE, DENSE, IO>(v, in, out, sh, t, c, active, tw,
+    tile_sync<NSYNC>();
+    col_stage<C, L, EPT, NC, DIR, P * RS, LOADK, MODE, ISTRIDE, OSTRIDE, DENSE, IO, NSYNC, BTG>(v, in, out, sh, t, c, active, tw,
                                                                                     scale, bt, n2, pitch, io);
   }
 }

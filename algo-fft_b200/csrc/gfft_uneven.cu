@@ -313,7 +313,7 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
     if (rows == 0) continue;
     C* work = static_cast<C*>(g.work);
     const C* tab = static_cast<const C*>(p->tab);
-    if (!g.bluestein && g.plan->algo == Algo::TwoPass && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
+    if (!g.bluestein && (g.plan->algo == Algo::TwoPass || g.plan->algo == Algo::L2Pipe) && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
       // one large length on the two-pass FFT: rows read and written in
       // place in the packed batch, no gather or scatter pass
       void* scratch = nullptr;
@@ -328,7 +328,7 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
       GFFT_CUDA(e);
       continue;
     }
-    if (g.bluestein && g.plan->algo == Algo::TwoPass && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
+    if (g.bluestein && (g.plan->algo == Algo::TwoPass || g.plan->algo == Algo::L2Pipe) && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
       // the chain fused into the two-pass FFT_M: rows read and written in
       // place in the packed batch, no gather or scatter pass
       void* scratch = nullptr;

@@ -651,6 +651,97 @@ def _convolve(dev, stream, iters, gen):
     return out
 
 
+CASES = ("pow2_cols", "uneven600", "bs_fused", "bs_tp", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
+         "gen_cols", "tp3t", "tp2", "p16384")
+
+
+def run_case(name: str, reps: int) -> int:
+    """One small workload of one kernel family, run `reps` times (profiling
+    runs: each case holds well under 1 GB on the device and launches its
+    kernel a handful of times).  Prints one line with the median device
+    time."""
+    import numpy as np
+    import torch
+    import algofft
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+
+    def cplx(n):
+        return torch.randn(2 * n, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+
+    close = []
+    if name == "pow2_cols":  # 4096 columns of length 1024 at stride 4096 (one 32 MB matrix)
+        n, cols = 1024, 4096
+        x, y = cplx(n * cols), None
+        y = torch.empty_like(x)
+        p = algofft.NewPlan(n)
+        close.append(p)
+        fn = lambda: p.StridedBatch(y, x, cols, cols, 1)  # noqa: E731
+    elif name == "uneven600":  # 600 transforms of the uneven workload's length mix
+        L = algofft.uneven_lengths(600, seed=1)
+        p = algofft.PlanUneven(L)
+        close.append(p)
+        x = cplx(p.Total())
+        y = torch.empty_like(x)
+        fn = lambda: p.Forward(y, x)  # noqa: E731
+    elif name in ("bs_fused", "bs_tp"):  # Bluestein: n = 8191 (M = 16384, one CTA) / 16411 (M = 65536)
+        n = 8191 if name == "bs_fused" else 16411
+        count = (1 << 27) // (8 * n)
+        x = cplx(n * count)
+        y = torch.empty_like(x)
+        p = algofft.NewPlan(n)
+        close.append(p)
+        fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
+    elif name == "conv_os":  # ConvolveReal, 8 signals of 2^20 reals with a 4097-tap kernel
+        cnt, na, nb = 8, 1 << 20, 4097
+        a = torch.rand(cnt * na, generator=gen, device=dev) * 2 - 1
+        k = torch.rand(nb, generator=gen, device=dev) * 2 - 1
+        d = torch.empty(cnt * (na + nb - 1), dtype=torch.float32, device=dev)
+        fn = lambda: algofft.ConvolveRealBatch(d, a, na, cnt, k)  # noqa: E731
+    elif name in ("c2r", "r2c"):  # real transforms, N = 4096, batch 8192
+        n, batch = 4096, 8192
+        xr = torch.rand(n * batch, generator=gen, device=dev) * 2 - 1
+        X = torch.empty(batch * (n // 2 + 1), dtype=torch.complex64, device=dev)
+        p = algofft.NewPlanRealWithOptions(n, algofft.PlanOptions(Batch=batch))
+        close.append(p)
+        p.Forward(X, xr)
+        fn = (lambda: p.Forward(X, xr)) if name == "r2c" else (lambda: p.Inverse(xr, X))
+    elif name == "mlp":  # the learned planner's training (Adam) and inference kernels
+        from algofft import planner
+        X = np.random.default_rng(0).standard_normal((4096, planner.sizes()[0])).astype(np.float32)
+        yv = np.random.default_rng(1).standard_normal(4096).astype(np.float32)
+        m = planner.Model(planner.init_params(0), planner.Model.norm_from(X, yv))
+        fn = lambda: (planner.train(X, yv, steps=200, chunk=200), m.predict(X))  # noqa: E731
+    elif name == "tc4096":  # tensor-core split-fp16 form, N = 4096, 8192 transforms
+        n, count = 4096, 8192
+        x = cplx(n * count)
+        y = torch.empty_like(x)
+        p = algofft.Plan(n, variant=f"gpu-sm100-tc16-n{n}")
+        close.append(p)
+        fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
+    elif name in ("l2p", "tp3t", "gen_cols", "tp2", "p16384"):
+        # L2-pipelined 2^20 (16 transforms, 16 MB groups), TMA three-pass 2^23 (4), runtime two-pass 50421
+        # (160), the default plan of 2^20 (split two-pass, 16), single pass 16384 (4096)
+        n, count, tok = {"l2p": (1 << 20, 16, "-l2p-1024x1024-c8x8-e16x16-s3-g16"), "tp3t": (1 << 23, 4, "-tp3t-"),
+                         "gen_cols": (50421, 160, "-mixed2-"), "tp2": (1 << 20, 16, None),
+                         "p16384": (16384, 4096, None)}[name]
+        x = cplx(n * count)
+        y = torch.empty_like(x)
+        toks = [t for t in algofft.Variants(n) if tok and tok in t]
+        p = algofft.Plan(n, variant=toks[0]) if tok else algofft.NewPlan(n)
+        close.append(p)
+        fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
+    else:
+        raise SystemExit(f"unknown case {name}; cases: {', '.join(CASES)}")
+    ms = _median_ms(fn, torch.cuda.current_stream(dev), reps)
+    for c in close:
+        c.Close()
+    print(json.dumps({"case": name, "reps": reps, "median_ms": ms}))
+    return 0
+
+
 def main():
     global SWEEP, BUF_BYTES
     ap = argparse.ArgumentParser()
@@ -664,9 +755,13 @@ def main():
     ap.add_argument("--extras", default=",".join(EXTRAS), help="comma-separated extras to run: " + ",".join(EXTRAS))
     ap.add_argument("--sizes", default="", help="comma-separated subset of lengths (profiling runs)")
     ap.add_argument("--batch-mib", type=int, default=BUF_BYTES >> 20, help="batch bytes per length in MiB")
+    ap.add_argument("--case", default="", help="run one small named workload (profiling): " + ",".join(CASES))
+    ap.add_argument("--reps", type=int, default=3, help="repetitions of --case")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.case:
+        return run_case(args.case, args.reps)
 
     import numpy as np
     import torch
