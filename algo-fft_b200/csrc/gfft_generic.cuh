@@ -56,10 +56,8 @@ __device__ __forceinline__ int gen_mod(int i, int p, float pinv, int& q) {
 // (shared memory, padded).  GI: the stage reads the transform's global
 // input `gin` instead of `in` (first stage); GO: it writes the global
 // output `gout` instead of `out`, scaled for the inverse (last stage).
-// Consecutive threads touch consecutive elements of both.  TWS: the
-// twiddle table `tw` sits in shared memory (generic loads) instead of
-// global memory (read-only cache loads).
-template <int R, int DIR, bool GI, bool GO, bool TWS = false, typename C>
+// Consecutive threads touch consecutive elements of both.
+template <int R, int DIR, bool GI, bool GO, typename C>
 __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* gout, typename RealOf<C>::type scale,
                                           int n, int p, float pinv, int T, int t, const C* __restrict__ tw) {
   const int nb = n / R;
@@ -73,10 +71,7 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* 
     }
     int q;
     const int k = gen_mod(i, p, pinv, q);
-    if (p > 1) {
-      if constexpr (TWS) apply_twiddles<R, DIR>(v, tw[k * step]);
-      else apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
-    }
+    if (p > 1) apply_twiddles<R, DIR>(v, __ldg(tw + k * step));
     dft<R, DIR>(v);
     const int j = q * p * R + k;
 #pragma unroll
@@ -92,19 +87,19 @@ __device__ __forceinline__ void gen_stage(const C* in, C* out, const C* gin, C* 
   }
 }
 
-template <int DIR, bool GI, bool GO, bool TWS = false, typename C>
+template <int DIR, bool GI, bool GO, typename C>
 __device__ __forceinline__ void gen_stage_any(int radix, const C* a, C* b, const C* gin, C* gout,
                                               typename RealOf<C>::type scale, int n, int p, float pi, int T, int t,
                                               const C* __restrict__ tw) {
   switch (radix) {
-    case 2: gen_stage<2, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 3: gen_stage<3, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 4: gen_stage<4, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 5: gen_stage<5, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 7: gen_stage<7, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 8: gen_stage<8, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    case 9: gen_stage<9, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
-    default: gen_stage<16, DIR, GI, GO, TWS>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 2: gen_stage<2, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 3: gen_stage<3, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 4: gen_stage<4, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 5: gen_stage<5, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 7: gen_stage<7, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 8: gen_stage<8, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    case 9: gen_stage<9, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
+    default: gen_stage<16, DIR, GI, GO>(a, b, gin, gout, scale, n, p, pi, T, t, tw); break;
   }
 }
 
@@ -112,12 +107,12 @@ __device__ __forceinline__ void gen_stage_any(int radix, const C* a, C* b, const
 // memory, padded layout; the caller synchronises after filling it), `b`
 // the other buffer.  Returns the buffer that holds the result, after a
 // barrier.
-template <int DIR, bool TWS = false, typename C>
+template <int DIR, typename C>
 __device__ __forceinline__ C* gen_fft(C* a, C* b, const GenSched& s, int t, const C* __restrict__ tw) {
   using Re = typename RealOf<C>::type;
   for (int st = 0; st < s.nst; ++st) {
-    gen_stage_any<DIR, false, false, TWS>(s.radix[st], a, b, static_cast<const C*>(nullptr),
-                                          static_cast<C*>(nullptr), Re(1), s.n, s.p[st], s.pinv[st], s.T, t, tw);
+    gen_stage_any<DIR, false, false>(s.radix[st], a, b, static_cast<const C*>(nullptr), static_cast<C*>(nullptr),
+                                     Re(1), s.n, s.p[st], s.pinv[st], s.T, t, tw);
     __syncthreads();
     C* tmp = a;
     a = b;
@@ -225,14 +220,10 @@ __global__ void __launch_bounds__(1024) k_gen_cols(const C* src, C* dst, int64_t
     }
     base[c * s.stride + gpad(row)] = v;
   }
-  // W_L once per CTA in shared memory, after the tile: every butterfly of
-  // every stage looks its twiddle up there
-  C* s_tw = base + NC * s.stride;
-  for (int i = tid; i < L; i += nthr) s_tw[i] = __ldg(tw + i);
   __syncthreads();
   const int slot = tid / s.T, t = tid % s.T;
   C* col = base + (slot < NC ? slot : 0) * s.stride;
-  gen_fft<DIR, true>(col, col + s.half, s, slot < NC ? t : kIdleThread, s_tw);
+  gen_fft<DIR>(col, col + s.half, s, slot < NC ? t : kIdleThread, tw);
   // every column's result sits in the same buffer of its region
   const C* res = base + ((s.nst & 1) ? s.half : 0);
   if (!valid) return;

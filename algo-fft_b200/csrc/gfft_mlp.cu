@@ -392,14 +392,17 @@ bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* toke
   std::lock_guard<std::mutex> g(M.mu);
   model_try_default();
   if (!M.loaded) return false;
-  const std::vector<std::string> toks = variant_tokens(prec, n);
-  if (toks.size() < 2) return false;
-  std::vector<float> xs(toks.size() * D);
-  for (size_t i = 0; i < toks.size(); ++i) {
-    float* f = &xs[i * D];
-    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, toks[i], f)) return false;
-    for (int d = 0; d < D; ++d) f[d] = (f[d] - M.norm[d]) / M.norm[D + d];
+  // candidates of a kind the model has no features for (variant families
+  // added after it was trained) are left out
+  std::vector<std::string> toks;
+  std::vector<float> xs;
+  for (const std::string& t : variant_tokens(prec, n)) {
+    float f[D];
+    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, t, f)) continue;
+    for (int d = 0; d < D; ++d) xs.push_back((f[d] - M.norm[d]) / M.norm[D + d]);
+    toks.push_back(t);
   }
+  if (toks.size() < 2) return false;
   std::vector<float> pred;
   if (!model_predict(xs, int(toks.size()), &pred)) return false;
   size_t best = 0;

@@ -132,7 +132,7 @@ static cudaError_t launch_cols(const GenSched& s, int dir, const void* src, void
   using Re = typename RealOf<C>::type;
   const int64_t tiles = (ncols + s.B - 1) / s.B;
   const int64_t blocks = tiles * count;
-  const size_t smem = (size_t(s.B) * s.stride + size_t(s.n)) * sizeof(C);  // tile + W_L table
+  const size_t smem = size_t(s.B) * s.stride * sizeof(C);
   if (blocks <= 0) return cudaSuccess;
   if (dir < 0)
     k_gen_cols<C, -1, MODE><<<unsigned(blocks), s.B * s.T, smem, st>>>(
@@ -196,14 +196,12 @@ gfft_status init_generic(PlanCore* c) {
   return GFFT_OK;
 }
 
-// Column-tile schedule of length L with up to `want` columns per tile (the
-// tile and the W_L table together within the shared-memory budget).
+// Column-tile schedule of length L with up to `want` columns per tile.
 static bool make_col_sched(int64_t L, size_t es, int want, GenSched* s) {
   if (!make_sched(L, s)) return false;
   int nc = want;
-  auto bytes = [&](int k) { return (size_t(k) * s->stride + size_t(L)) * es; };
-  while (nc > 1 && (bytes(nc) > size_t(kSmemBudget) || nc * s->T > 1024)) nc /= 2;
-  if (bytes(nc) > size_t(kSmemBudget) || nc * s->T > 1024) return false;
+  while (nc > 1 && (size_t(nc) * s->stride * es > size_t(kSmemBudget) || nc * s->T > 1024)) nc /= 2;
+  if (size_t(nc) * s->stride * es > size_t(kSmemBudget) || nc * s->T > 1024) return false;
   s->B = nc;
   return true;
 }

@@ -33,31 +33,16 @@ __device__ __forceinline__ C chirp_of(const C* w, int64_t m) {
   else return v;
 }
 
-// chirp-weighted, zero-padded input: m = row * N2 + col0 + c.  The pad
-// boundary is taken once per column: rows below rlim(c) hold input, the
-// rest are zero (no 64-bit index test per element).
+// chirp-weighted, zero-padded input: m = row * N2 + col0 + c
 template <typename C, int UDIR>
 struct BsChirpIn {
   const C* x;  // this transform's input
   const C* w;
   int64_t n, n2, col0;
-  __device__ __forceinline__ int rlim(int c) const {
-    const int64_t left = n - col0 - c;  // input elements at or after column c of row 0
-    return left <= 0 ? 0 : int((left + n2 - 1) / n2);
-  }
-  __device__ __forceinline__ C load(int row, int c, int lim) const {
-    if (row >= lim) return C{0, 0};
+  __device__ __forceinline__ C load(int row, int c) const {
     const int64_t m = int64_t(row) * n2 + col0 + c;
-    return cmul(ld_stream(x + m), chirp_of<UDIR>(w, m));
+    return m < n ? cmul(ld_stream(x + m), chirp_of<UDIR>(w, m)) : C{0, 0};
   }
-};
-
-// The IO object col_stage sees: the column's row limit fixed at construction.
-template <typename C, int UDIR>
-struct BsChirpInCol {
-  BsChirpIn<C, UDIR> in;
-  int lim;
-  __device__ __forceinline__ C load(int row, int c) const { return in.load(row, c, lim); }
 };
 
 // spectrum times the filter, k = col0 + c + N1 * row, kept in L2 for the
@@ -189,10 +174,9 @@ k_bs_tp(BsTpParams p, int64_t b0) {
     const bool active = tid < S1::TPB;
     const int c = tid % NC1, t = tid / NC1;
     const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
-    const BsChirpIn<C, UDIR> cin{rw.x, rw.w, rw.n, N2, col0};
-    const BsChirpInCol<C, UDIR> io{cin, cin.rlim(c)};
+    const BsChirpIn<C, UDIR> io{rw.x, rw.w, rw.n, N2, col0};
     C* y = scratch + bl * TP::N;
-    col_stage<C, N1, EPT1, NC1, -1, 1, LOAD_FN, OUT_SMEM_TWIDDLE, N2, 0, false, BsChirpInCol<C, UDIR>>(
+    col_stage<C, N1, EPT1, NC1, -1, 1, LOAD_FN, OUT_SMEM_TWIDDLE, N2, 0, false, BsChirpIn<C, UDIR>>(
         v, nullptr, nullptr, sh, t, c, active, static_cast<const C*>(p.tw1), Re(1), p.bt, int64_t(col0 + c), 0,
         io);
     for (int e = tid; e < N1 * NC1; e += TP::TPB) {
