@@ -20,82 +20,11 @@
 #include <mutex>
 #include <thread>
 #include <vector>
+#include "gfft_copypool.h"
 #include "gfft_internal.h"
 
 namespace gfft {
 namespace {
-
-// Splits large memcpys over a few persistent threads (one call at a time;
-// the calling thread takes a share too).
-class CopyPool {
- public:
-  static CopyPool& get() {
-    static CopyPool* pool = new CopyPool();  // never destroyed: workers outlive static teardown
-    return *pool;
-  }
-
-  void copy(void* dst, const void* src, size_t bytes) {
-    constexpr size_t kPart = size_t(1) << 20;
-    if (bytes <= 2 * kPart || workers_.empty()) {
-      std::memcpy(dst, src, bytes);
-      return;
-    }
-    std::lock_guard<std::mutex> one(call_mu_);
-    {
-      std::lock_guard<std::mutex> g(mu_);
-      dst_ = static_cast<char*>(dst);
-      src_ = static_cast<const char*>(src);
-      bytes_ = bytes;
-      part_ = std::max(kPart, (bytes / (workers_.size() + 1) + 4095) & ~size_t(4095));
-      next_.store(0);
-      busy_ = workers_.size();
-      ++gen_;
-    }
-    cv_.notify_all();
-    run_parts();
-    std::unique_lock<std::mutex> g(mu_);
-    done_cv_.wait(g, [&] { return busy_ == 0; });
-  }
-
- private:
-  CopyPool() {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned n = std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
-    for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
-    for (auto& t : workers_) t.detach();
-  }
-
-  void run_parts() {
-    for (;;) {
-      const size_t at = next_.fetch_add(part_);
-      if (at >= bytes_) return;
-      std::memcpy(dst_ + at, src_ + at, std::min(part_, bytes_ - at));
-    }
-  }
-
-  void loop() {
-    uint64_t seen = 0;
-    for (;;) {
-      {
-        std::unique_lock<std::mutex> g(mu_);
-        cv_.wait(g, [&] { return gen_ != seen; });
-        seen = gen_;
-      }
-      run_parts();
-      std::lock_guard<std::mutex> g(mu_);
-      if (--busy_ == 0) done_cv_.notify_all();
-    }
-  }
-
-  std::vector<std::thread> workers_;
-  std::mutex call_mu_, mu_;
-  std::condition_variable cv_, done_cv_;
-  char* dst_ = nullptr;
-  const char* src_ = nullptr;
-  size_t bytes_ = 0, part_ = 0, busy_ = 0;
-  std::atomic<size_t> next_{0};
-  uint64_t gen_ = 0;
-};
 
 // Pinned staging buffers kept for later calls (portable: any device may
 // copy from them); one lane set per concurrent call.
@@ -145,27 +74,87 @@ bool host_pinned(const void* p) {
 
 constexpr int kLanes = 3;
 
+// Streams and events of the lanes, created once per device and reused by
+// later calls (one set per concurrent call).
+struct LaneSet {
+  int dev = -1;
+  bool busy = false;
+  cudaStream_t st[kLanes] = {};
+  cudaEvent_t ev[kLanes] = {};
+};
+
+class LanePool {
+ public:
+  static LanePool& get() {
+    static LanePool* pool = new LanePool();
+    return *pool;
+  }
+  cudaError_t acquire(int dev, LaneSet** out) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      for (LaneSet* l : sets_)
+        if (l->dev == dev && !l->busy) {
+          l->busy = true;
+          *out = l;
+          return cudaSuccess;
+        }
+    }
+    auto* l = new LaneSet();
+    l->dev = dev;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&l->st[i], cudaStreamNonBlocking);
+    for (int i = 0; i < kLanes && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&l->ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      for (int i = 0; i < kLanes; ++i) {
+        if (l->st[i]) cudaStreamDestroy(l->st[i]);
+        if (l->ev[i]) cudaEventDestroy(l->ev[i]);
+      }
+      delete l;
+      return e;
+    }
+    l->busy = true;
+    std::lock_guard<std::mutex> g(mu_);
+    sets_.push_back(l);
+    *out = l;
+    return cudaSuccess;
+  }
+  void release(LaneSet* l) {
+    std::lock_guard<std::mutex> g(mu_);
+    l->busy = false;
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<LaneSet*> sets_;
+};
+
 }  // namespace
 
 gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t count) {
   DeviceGuard dg;
   GFFT_CUDA(dg.set(p->core.device));
   const size_t tb = size_t(p->core.n) * elem_bytes(p->core.prec);
-  const bool staged = !(host_pinned(src) && host_pinned(dst));
-  // chunks of about 64 MB (pinned) / 32 MB (staged), whole transforms
-  const size_t target = staged ? (size_t(32) << 20) : (size_t(64) << 20);
+  const size_t total = size_t(count) * tb;
+  // tiny batches (up to 64 KB) copy straight from the caller's memory (the
+  // driver stages them); anything larger in pageable memory goes through
+  // the pinned lanes and the copy pool
+  const bool staged = total > (size_t(64) << 10) && !(host_pinned(src) && host_pinned(dst));
+  // chunks of about 64 MB (pinned) / 32 MB (staged), whole transforms; a
+  // smaller batch is cut into about six chunks so the lanes still overlap
+  const size_t target = std::min(staged ? (size_t(32) << 20) : (size_t(64) << 20),
+                                 std::max(size_t(256) << 10, total / 6));
   const int64_t per = std::max<int64_t>(1, std::min<int64_t>(count, int64_t(target / tb)));
   const int64_t nchunks = (count + per - 1) / per;
   const int lanes = int(std::min<int64_t>(kLanes, nchunks));
-  cudaStream_t st[kLanes] = {};
-  cudaEvent_t ev[kLanes] = {};
+  LaneSet* ls = nullptr;
+  GFFT_CUDA(LanePool::get().acquire(p->core.device, &ls));
+  cudaStream_t* st = ls->st;
+  cudaEvent_t* ev = ls->ev;
   void* d[kLanes] = {};
   void* h[kLanes] = {};
   int64_t pending[kLanes] = {-1, -1, -1};  // chunk whose result waits in lane's pinned buffer
   gfft_status s = GFFT_OK;
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
-  for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
   for (int i = 0; i < lanes && e == cudaSuccess; ++i) e = ws_alloc(&d[i], size_t(per) * tb, st[i]);
   for (int i = 0; staged && i < lanes && e == cudaSuccess; ++i) e = PinnedPool::get().acquire(size_t(per) * tb, &h[i]);
   if (e != cudaSuccess) s = cuda_status(e, "host path setup");
@@ -212,14 +201,12 @@ gfft_status run_host(gfft_plan* p, int dir, void* dst, const void* src, int64_t 
   // results of the last chunks, oldest first
   for (int64_t k = std::max<int64_t>(0, nchunks - lanes); k < nchunks && s == GFFT_OK; ++k) s = drain(int(k % lanes));
   for (int i = 0; i < lanes; ++i) {
-    if (!st[i]) continue;
     if (d[i]) cudaFreeAsync(d[i], st[i]);
     e = cudaStreamSynchronize(st[i]);
     if (e != cudaSuccess && s == GFFT_OK) s = cuda_status(e, "cudaStreamSynchronize");
-    cudaStreamDestroy(st[i]);
-    if (ev[i]) cudaEventDestroy(ev[i]);
     PinnedPool::get().release(h[i]);
   }
+  LanePool::get().release(ls);
   return s;
 }
 

@@ -78,6 +78,8 @@ struct PlanCore {
   // cannot address): kernels, group bytes in MB and scratch slots
   const L2PipeKernel* l2[2] = {nullptr, nullptr};
   int l2_gmb = 16, l2_slots = 3;
+  // tensor-core form: radix of its leading FP32 stage (1: n is a power of 16)
+  int tc_lead = 1;
   unsigned* status = nullptr;  // device word: nonzero once a bounded wait expired
   // runtime-schedule (7-smooth) plans
   GenSched gs{}, gs1{}, gs2{};
@@ -98,7 +100,8 @@ gfft_status init_generic(PlanCore* c);
 std::vector<std::string> mixed_tokens(int prec, int64_t n);
 gfft_status init_gen_twopass(PlanCore* c);
 gfft_status init_bluestein(PlanCore* c);
-// Tensor-core split-fp16 radix-16 form (complex64, n = 16^s, 16 <= n <= 2^24).
+// Tensor-core split-fp16 radix-16 form (complex64, powers of two 16 <= n <= 2^24;
+// n = r * 16^s with r = 2, 4, 8 takes one leading FP32 radix-r stage).
 bool tc_supported(int64_t n);
 gfft_status init_tc(PlanCore* c);
 gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,

@@ -29,6 +29,13 @@
 // 4096 whose transforms k_tc_fft finishes, writing each output to its
 // natural index (block digits reversed).
 //
+// Powers of two that are not powers of 16, n = r 16^s (r = 2, 4, 8), first
+// run one decimation-in-frequency stage of radix r in FP32 on the CUDA cores
+// (k_tc_lead: block j of a transform gets sum_i x[m + i n/r] W_r^{ij} times
+// W_n^{jm}), then the radix-16 tensor-core chain on each block of n/r
+// points; k_tc_fft's output index then reverses the block digits in the
+// mixed base (r for the leading digit, 16 for the rest).
+//
 // The CUDA-core FP32 path (k_pow2 / k_tp_split) stays the default; this form
 // is selected per plan by its variant token "gpu-sm100-tc16-n<N>"
 // (gfft_plan_new_variant; the planner never picks it on its own) and is
@@ -269,12 +276,14 @@ __device__ __forceinline__ void tmem_free(TcState& st, unsigned* status) {
 
 // Transforms of length N = 16^S (S <= 3): CTA c owns elements
 // [c * 4096, c * 4096 + 4096) of the batch viewed as units of N; with nb > 1
-// (N = 4096 finishing a larger transform of nb * 4096 points) each unit is
-// block `blk` of its transform and output k goes to blk' + nb * k, blk' the
-// digit-reversed block index (dig base-16 digits).
+// (N finishing a larger transform of nb * N points) each unit is block
+// `blk` of its transform and output k goes to blk' + nb * k, blk' the
+// digit-reversed block index: blk = j * 16^dig + d with j < lead (the block
+// of a leading radix-`lead` stage, 0 without one) and d of dig base-16
+// digits; blk' = j + lead * reverse16(d).
 template <int DIR>
 __global__ void __launch_bounds__(256) k_tc_fft(const float2* __restrict__ src, float2* __restrict__ dst,
-                                                 int64_t units, int N, int S, int64_t nb, int dig,
+                                                 int64_t units, int N, int S, int64_t nb, int dig, int lead,
                                                  const float2* __restrict__ tw, float scale, unsigned* status) {
   extern __shared__ __align__(128) unsigned char sm[];
   float2* x = reinterpret_cast<float2*>(sm + SM_X);
@@ -314,15 +323,17 @@ __global__ void __launch_bounds__(256) k_tc_fft(const float2* __restrict__ src, 
         for (int r = 0; r < R; ++r) st_stream(out + base + r * P, make_float2(y[r].x * scale, y[r].y * scale));
       } else {
         const int64_t tr = unit / nb, blk = unit % nb;
-        int64_t rev = 0, q = blk;
+        const int64_t nsub = nb / lead;  // 16^dig
+        int64_t rev = 0, q = blk % nsub;
         for (int d = 0; d < dig; ++d) {
           rev = rev * R + q % R;
           q /= R;
         }
+        rev = blk / nsub + lead * rev;
         float2* out = dst + tr * nb * N + rev;
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-          st_stream(out + int64_t(base + r * P) * nb, make_float2(y[r].x * scale, y[r].y * scale));
+        for (int r = 0; r < R; ++r)  // index within the unit times the block count
+          st_stream(out + int64_t(base - b * N + r * P) * nb, make_float2(y[r].x * scale, y[r].y * scale));
       }
     }
     P *= R;
@@ -362,21 +373,41 @@ __global__ void __launch_bounds__(256) k_tc_dif(const float2* __restrict__ src, 
   tmem_free(st, status);
 }
 
+// Leading decimation-in-frequency stage of radix RL (2, 4 or 8) in FP32 on
+// the CUDA cores, for n = RL * Lp: output block j of a transform holds
+// sum_i x[m + i Lp] W_RL^{ij} times W_n^{jm} at j Lp + m.  Consecutive
+// threads take consecutive m, so every load and store is coalesced.
+template <int RL, int DIR>
+__global__ void k_tc_lead(const float2* __restrict__ src, float2* __restrict__ dst, int64_t total, int64_t Lp,
+                          BigTwiddle bt) {
+  for (int64_t g = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < total; g += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t m = g % Lp, base = (g / Lp) * Lp * RL;
+    float2 v[RL];
+#pragma unroll
+    for (int i = 0; i < RL; ++i) v[i] = ld_stream(src + base + m + i * Lp);
+    dft<RL, DIR>(v);
+    st_stream(dst + base + m, v[0]);
+#pragma unroll
+    for (int j = 1; j < RL; ++j) st_stream(dst + base + j * Lp + m, cmul(v[j], big_twiddle<float2, DIR>(bt, j * m)));
+  }
+}
+
 }  // namespace tc
 
-bool tc_supported(int64_t n) {
-  if (n < 16) return false;
-  int s = 0;
-  while (n > 1 && n % 16 == 0) {
-    n /= 16;
-    ++s;
-  }
-  return n == 1 && s >= 1 && s <= 6;
+// Radix of the leading FP32 stage of n in the tensor-core form (1 for a
+// power of 16), 0 when the form cannot serve n.
+static int tc_lead_of(int64_t n) {
+  if (n < 16 || n > (int64_t(1) << 24) || (n & (n - 1))) return 0;
+  int lg = 0;
+  while ((int64_t(1) << lg) < n) ++lg;
+  return 1 << (lg % 4);
 }
+
+bool tc_supported(int64_t n) { return tc_lead_of(n) != 0; }
 
 gfft_status init_tc(PlanCore* c) {
   if (c->prec != kC64 || !tc_supported(c->n)) {
-    set_error("the tensor-core form serves complex64 lengths 16^s, 16 <= n <= 2^24");
+    set_error("the tensor-core form serves complex64 powers of two 16 <= n <= 2^24");
     return GFFT_ERR_NOT_IMPLEMENTED;
   }
   static cudaError_t attr = [] {
@@ -390,27 +421,57 @@ gfft_status init_tc(PlanCore* c) {
     return e;
   }();
   GFFT_CUDA(attr);
-  // tables: W_n' for every stage length used (n' = n, n/16, ..., and 4096 or n)
+  // tables: W_L for every radix-16 stage length used (L = n / lead, /16, ...,
+  // and 4096 or less for the last kernel), then for a leading stage the
+  // split table of W_n (hi[a] lo[b], m = a 2^shift + b)
   const int64_t n = c->n;
+  const int lead = tc_lead_of(n);
+  const int64_t lp = n / lead;
   int64_t total = 0;
-  for (int64_t L = n; L > 4096; L /= 16) total += L;
-  const int64_t nf = std::min<int64_t>(n, 4096);
+  for (int64_t L = lp; L > 4096; L /= 16) total += L;
+  const int64_t nf = std::min<int64_t>(lp, 4096);
   total += nf;
+  int lg = 0;
+  while ((int64_t(1) << lg) < n) ++lg;
+  const int shift = (lg + 1) / 2;
+  const int64_t nlo = int64_t(1) << shift, nhi = n >> shift;
+  if (lead > 1) total += nlo + nhi;
   GFFT_CUDA(cudaMalloc(&c->tw, size_t(total) * 8));
   int64_t off = 0;
-  for (int64_t L = n; L > 4096; L /= 16) {
+  for (int64_t L = lp; L > 4096; L /= 16) {
     gfft_status s = fill_twiddles(kC64, static_cast<char*>(c->tw) + off * 8, L, L, 1, 0);
     if (s != GFFT_OK) return s;
     off += L;
   }
   gfft_status s = fill_twiddles(kC64, static_cast<char*>(c->tw) + off * 8, nf, nf, 1, 0);
   if (s != GFFT_OK) return s;
+  off += nf;
+  if (lead > 1) {
+    char* base = static_cast<char*>(c->tw);
+    s = fill_twiddles(kC64, base + off * 8, n, nlo, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(kC64, base + (off + nlo) * 8, n, nhi, nlo, 0);
+    if (s != GFFT_OK) return s;
+    c->bt_lo = base + off * 8;
+    c->bt_hi = base + (off + nlo) * 8;
+    c->bt_shift = shift;
+  }
+  c->tc_lead = lead;
   GFFT_CUDA(cudaMalloc(&c->status, sizeof(unsigned)));
   GFFT_CUDA(cudaMemset(c->status, 0, sizeof(unsigned)));
   GFFT_CUDA(cudaStreamSynchronize(0));
   c->algo = Algo::TensorCore;
   c->name = "gpu-sm100-tc16-n" + std::to_string(n);
   return GFFT_OK;
+}
+
+template <int DIR>
+static cudaError_t launch_lead(int lead, const float2* in, float2* out, int64_t total, int64_t lp, BigTwiddle bt,
+                               cudaStream_t st) {
+  const unsigned blocks = unsigned(std::min<int64_t>((total + 255) / 256, 148 * 32));
+  if (lead == 2) tc::k_tc_lead<2, DIR><<<blocks, 256, 0, st>>>(in, out, total, lp, bt);
+  else if (lead == 4) tc::k_tc_lead<4, DIR><<<blocks, 256, 0, st>>>(in, out, total, lp, bt);
+  else tc::k_tc_lead<8, DIR><<<blocks, 256, 0, st>>>(in, out, total, lp, bt);
+  return cudaGetLastError();
 }
 
 gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int64_t count, int64_t idist,
@@ -420,25 +481,32 @@ gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int6
     set_error("the tensor-core form takes contiguous batches");
     return GFFT_ERR_NOT_IMPLEMENTED;
   }
+  const int lead = c->tc_lead;
+  const int64_t lp = n / lead;
   const float scale = dir < 0 ? 1.f : float(1.0 / double(n));
   const float2* in = static_cast<const float2*>(src);
   float2* out = static_cast<float2*>(dst);
   const float2* tw = static_cast<const float2*>(c->tw);
-  if (n <= 4096) {
-    int S = 0;
-    for (int64_t m = n; m > 1; m /= 16) ++S;
+  // the last kernel's unit: blocks of 4096 points, or the whole n / lead
+  const int64_t nu = std::min<int64_t>(lp, 4096);
+  int S = 0;
+  for (int64_t m = nu; m > 1; m /= 16) ++S;
+  if (lead == 1 && n <= 4096) {
     const int64_t blocks = (count * n + tc::ELEMS - 1) / tc::ELEMS;
     if (dir < 0)
-      tc::k_tc_fft<-1><<<unsigned(blocks), 256, tc::SM_TOTAL, st>>>(in, out, count, int(n), S, 1, 0, tw, scale, c->status);
+      tc::k_tc_fft<-1><<<unsigned(blocks), 256, tc::SM_TOTAL, st>>>(in, out, count, int(n), S, 1, 0, 1, tw, scale,
+                                                                    c->status);
     else
-      tc::k_tc_fft<1><<<unsigned(blocks), 256, tc::SM_TOTAL, st>>>(in, out, count, int(n), S, 1, 0, tw, scale, c->status);
+      tc::k_tc_fft<1><<<unsigned(blocks), 256, tc::SM_TOTAL, st>>>(in, out, count, int(n), S, 1, 0, 1, tw, scale,
+                                                                   c->status);
     GFFT_CUDA(cudaGetLastError());
     return GFFT_OK;
   }
-  // DIF stages over HBM, ping-pong between two scratch halves (never
-  // through dst, so src == dst is safe); k_tc_fft then writes dst
-  int stages = 0;
-  for (int64_t L = n; L > 4096; L /= 16) ++stages;
+  // stages over HBM (the leading FP32 stage, then radix-16 DIF stages down
+  // to blocks of 4096), ping-pong between two scratch halves (never through
+  // dst, so src == dst is safe); k_tc_fft then writes dst
+  int stages = lead > 1 ? 1 : 0;
+  for (int64_t L = lp; L > 4096; L /= 16) ++stages;
   const size_t half_bytes = size_t(count) * size_t(n) * 8;
   void* ws = nullptr;
   GFFT_CUDA(ws_alloc(&ws, half_bytes * (stages > 1 ? 2 : 1), st));
@@ -447,7 +515,18 @@ gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int6
   int which = 0, dig = 0;
   int64_t off = 0;
   cudaError_t e = cudaSuccess;
-  for (int64_t L = n; L > 4096 && e == cudaSuccess; L /= 16, ++dig) {
+  if (lead > 1) {
+    BigTwiddle bt;
+    bt.lo = c->bt_lo;
+    bt.hi = c->bt_hi;
+    bt.shift = c->bt_shift;
+    float2* nxt = bufs[which];
+    e = dir < 0 ? launch_lead<-1>(lead, cur, nxt, count * lp, lp, bt, st)
+                : launch_lead<1>(lead, cur, nxt, count * lp, lp, bt, st);
+    cur = nxt;
+    which ^= 1;
+  }
+  for (int64_t L = lp; L > 4096 && e == cudaSuccess; L /= 16, ++dig) {
     float2* nxt = bufs[which];
     const int64_t bf = count * (n / 16);
     const unsigned blocks = unsigned((bf + tc::BPC - 1) / tc::BPC);
@@ -461,13 +540,14 @@ gfft_status exec_tc(const PlanCore* c, int dir, void* dst, const void* src, int6
     which ^= 1;
   }
   if (e == cudaSuccess) {
-    const int64_t nb = n / 4096, units = count * nb;
+    const int64_t nb = n / nu, units = count * nb;
+    const unsigned blocks = unsigned((units * nu + tc::ELEMS - 1) / tc::ELEMS);
     if (dir < 0)
-      tc::k_tc_fft<-1><<<unsigned(units), 256, tc::SM_TOTAL, st>>>(cur, out, units, 4096, 3, nb, dig, tw + off, scale,
-                                                                   c->status);
+      tc::k_tc_fft<-1><<<blocks, 256, tc::SM_TOTAL, st>>>(cur, out, units, int(nu), S, nb, dig, lead, tw + off, scale,
+                                                          c->status);
     else
-      tc::k_tc_fft<1><<<unsigned(units), 256, tc::SM_TOTAL, st>>>(cur, out, units, 4096, 3, nb, dig, tw + off, scale,
-                                                                  c->status);
+      tc::k_tc_fft<1><<<blocks, 256, tc::SM_TOTAL, st>>>(cur, out, units, int(nu), S, nb, dig, lead, tw + off, scale,
+                                                         c->status);
     e = cudaGetLastError();
   }
   cudaFreeAsync(ws, st);

@@ -1,7 +1,9 @@
 """Tensor-core precision form (split fp16 hi+lo operands, FP32 accumulation
 on tcgen05.mma) against the FP64 FFT: the stated complex64 tolerance,
 rel L2 <= 1e-6 * log2 N, on both input sets of the precision comparison
-(i.i.d. N(0,1), and log-uniform magnitudes 1e-4..1e4 with uniform phase)."""
+(i.i.d. N(0,1), and log-uniform magnitudes 1e-4..1e4 with uniform phase).
+Powers of two that are not powers of 16 (n = r * 16^s, r = 2, 4, 8) run a
+leading FP32 radix-r stage before the radix-16 tensor-core stages."""
 import numpy as np
 import pytest
 
@@ -23,7 +25,8 @@ def _tc(n):
     return algofft.Plan(n, algofft.COMPLEX64, variant=f"gpu-sm100-tc16-n{n}")
 
 
-@pytest.mark.parametrize("n", [16, 256, 4096, 65536, 1 << 20, 1 << 24])
+@pytest.mark.parametrize("n", [16, 32, 64, 256, 512, 2048, 4096, 8192, 65536, 1 << 17, 1 << 20, 1 << 21,
+                               1 << 22, 1 << 23, 1 << 24])
 @pytest.mark.parametrize("kind", ["normal", "loguniform"])
 def test_tc_forward_inverse(n, kind):
     import torch
@@ -46,7 +49,8 @@ def test_tc_forward_inverse(n, kind):
     assert rel_l2(bh, x) <= 2 * tol_c2c(n, False)
 
 
-@pytest.mark.parametrize("n,count", [(16, 100), (256, 3), (4096, 1), (65536, 1)])
+@pytest.mark.parametrize("n,count", [(16, 100), (32, 77), (256, 3), (4096, 1), (8192, 3), (65536, 1),
+                                     (1 << 21, 1)])
 def test_tc_ragged_batch_and_in_place(n, count):
     import torch
     x = _inputs("normal", n * count, seed=count)
@@ -63,6 +67,6 @@ def test_tc_ragged_batch_and_in_place(n, count):
 
 
 def test_tc_rejects_other_lengths():
-    for n in (8, 32, 1024, 12288):
+    for n in (2, 8, 12288, 1000, 1 << 25):
         with pytest.raises(algofft.ErrNotImplemented):
             _tc(n)
