@@ -916,7 +916,7 @@ def main():
             "per_size_gbs": {str(n): bytes_per_transform(n) * bufs[n][2] * args.steps / (per_size_ms[n] / 1e3) / 1e9
                              for n in SWEEP},
             "per_size_transforms_per_s": {str(n): bufs[n][2] * args.steps / (per_size_ms[n] / 1e3) for n in SWEEP},
-            "transforms_per_s": sum(bufs[n][2] for n in SWEEP) * args.steps / (dev_ms / 1e3),
+            "transforms_per_s": world * sum(bufs[n][2] for n in SWEEP) * args.steps / (dev_ms / 1e3),
             "rel_l2_vs_fp64": {str(n): errs[n] for n in SWEEP},
             "tolerance": "rel L2 <= 1e-6*log2(N) (complex64)",
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
