@@ -91,3 +91,66 @@ def test_known_answers_at_scale(n):
         assert err <= bound, (alg, name, err, bound)
         rel = np.linalg.norm(g - want) / np.linalg.norm(want)
         assert rel <= factor * tol_c2c(m, False), (alg, name, rel)
+
+
+@pytest.mark.parametrize("n", [4096, 1 << 16, 1 << 20, 50421, 16411])
+def test_known_answers_at_scale_c128(n):
+    """The same signals in complex128 against the 1e-13 * log2 N bound."""
+    import torch
+    rows = _rows(n)
+    x = np.concatenate([r[1] for r in rows])
+    with algofft.NewPlan64(n) as p:
+        src = torch.from_numpy(x).cuda()
+        y = torch.empty_like(src)
+        p.ForwardBatch(y, src, len(rows))
+        torch.cuda.synchronize()
+        got = y.cpu().numpy().reshape(len(rows), n)
+        alg = p.Algorithm()
+    bluestein = alg.startswith("gpu-sm100-bluestein")
+    m = 1 << (2 * n - 2).bit_length() if bluestein else n
+    factor = 2.0 if bluestein else 1.0
+    for (name, xin, want), g in zip(rows, got):
+        size = max(np.linalg.norm(xin), np.max(np.abs(want)))
+        err = np.max(np.abs(g - want))
+        assert err <= factor * 1e-13 * math.log2(m) * size, (alg, name, err)
+        assert np.linalg.norm(g - want) / np.linalg.norm(want) <= factor * tol_c2c(m, True), (alg, name)
+
+
+@pytest.mark.parametrize("n", [4096, 1 << 16, 1 << 20, 6000, 100000])
+def test_known_answers_real_at_scale(n):
+    """R2C of the reference's real signals (plan_real_test.go:14-161:
+    impulse -> all ones, constant c -> n c at bin 0, cos(2 pi f j / n) ->
+    n/2 at bin f) at large n, checked bin by bin against the closed forms,
+    then C2R back to the signal."""
+    import torch
+    k = np.arange(n, dtype=np.int64)
+    h = n // 2 + 1
+    f = 10
+    sigs, specs = [], []
+    x = np.zeros(n)
+    x[0] = 1.0
+    sigs.append(("impulse", x))
+    specs.append(np.ones(h, np.complex128))
+    sigs.append(("constant", np.full(n, 2.0)))
+    X = np.zeros(h, np.complex128)
+    X[0] = 2.0 * n
+    specs.append(X)
+    sigs.append(("cosine", np.cos(2 * np.pi * ((f * k) % n) / n)))
+    X = np.zeros(h, np.complex128)
+    X[f] = n / 2
+    specs.append(X)
+    xr = np.concatenate([s[1] for s in sigs]).astype(np.float32)
+    with algofft.NewPlanRealWithOptions(n, algofft.PlanOptions(Batch=len(sigs))) as p:
+        src = torch.from_numpy(xr).cuda()
+        spec = torch.empty(len(sigs) * h, dtype=torch.complex64, device="cuda")
+        p.Forward(spec, src)
+        back = torch.empty_like(src)
+        p.Inverse(back, spec)
+        torch.cuda.synchronize()
+        got = spec.cpu().numpy().astype(np.complex128).reshape(len(sigs), h)
+        rt = back.cpu().numpy().astype(np.float64).reshape(len(sigs), n)
+    for (name, xin), want, g, r in zip(sigs, specs, got, rt):
+        size = max(np.linalg.norm(xin), np.max(np.abs(want)))
+        err = np.max(np.abs(g - want))
+        assert err <= max(1e-3, 2e-6 * math.log2(n) * size), (name, err)
+        assert np.max(np.abs(r - xin)) <= max(1e-5, 4e-6 * math.log2(n) * np.max(np.abs(xin))), name
