@@ -27,7 +27,8 @@ namespace gfft {
 namespace {
 
 // Pinned staging buffers kept for later calls (portable: any device may
-// copy from them); one lane set per concurrent call.
+// copy from them); one lane set per concurrent call.  At most kKeep bytes
+// wait in the free list; a buffer released beyond that is freed.
 class PinnedPool {
  public:
   static PinnedPool& get() {
@@ -40,6 +41,7 @@ class PinnedPool {
       auto it = free_.lower_bound(bytes);
       if (it != free_.end() && it->first <= 2 * bytes) {
         *out = it->second;
+        kept_ -= it->first;
         free_.erase(it);
         return cudaSuccess;
       }
@@ -53,14 +55,25 @@ class PinnedPool {
   }
   void release(void* p) {
     if (!p) return;
-    std::lock_guard<std::mutex> g(mu_);
-    free_.emplace(size_of_[p], p);
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      const size_t b = size_of_[p];
+      if (kept_ + b <= kKeep) {
+        free_.emplace(b, p);
+        kept_ += b;
+        return;
+      }
+      size_of_.erase(p);
+    }
+    cudaFreeHost(p);
   }
 
  private:
+  static constexpr size_t kKeep = size_t(512) << 20;
   std::mutex mu_;
   std::multimap<size_t, void*> free_;
   std::map<void*, size_t> size_of_;
+  size_t kept_ = 0;  // bytes in free_
 };
 
 bool host_pinned(const void* p) {
