@@ -43,11 +43,16 @@ WORKLOAD = "c64 C2C ForwardBatch power-of-two sweep N=2^4..2^24, 1 GiB batch per
 
 # DRAM bytes per transform (read + write, all passes) of the multi-pass
 # plans, each the sum of dram__bytes_read.sum and dram__bytes_write.sum over
-# the passes of one ncu capture of a 16-transform batch of that plan, divided
-# by 16; used to scale `roofline.traffic` to a launch.
+# the passes of one ncu capture of a small batch of that plan (16
+# transforms, or 256 MiB), divided by its transform count; used to scale
+# `roofline.traffic` to a launch.
 TRAFFIC_PER_TRANSFORM = {"gpu-sm100-tp-4096x4096-t16384-e16": 490.6e6,
                          "gpu-sm100-tp3-256x256x128": 359.4e6,
-                         "gpu-sm100-tp3t-256x256x128-t4096-e16-s3": 363.4e6}
+                         "gpu-sm100-tp3t-256x256x128-t4096-e16-s3": 363.4e6,
+                         "gpu-sm100-tp-1024x1024-t8192-e16": 30.77e6,
+                         "gpu-sm100-tp-1024x2048-t8192-e16": 61.69e6,
+                         "gpu-sm100-tp3t-256x128x128-t4096-e16-s3": 179.92e6,
+                         "gpu-sm100-tp3-256x256x256": 715.25e6}
 
 
 def launches_of(algorithm: str, count: int, n: int, es: int) -> int:
