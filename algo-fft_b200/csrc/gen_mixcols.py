@@ -1,0 +1,119 @@
+"""Writes kernels_mixcols_t0.cu .. kernels_mixcols_t7.cu: the compiled
+mixed-radix column tiles (gfft_mixcols.cuh) of every 7-smooth column length
+48 <= L <= 1024, spread over eight files so nvcc builds them in parallel.
+
+Schedule rule, from timing the candidates on a B200 (two stages against three
+and four, several tile widths and occupancies, at L = 100..1000):
+  * two stages L = a * b, the larger radix a first and as small as it can be
+    (both radices 7-smooth, at most 49, or a power of two up to 64): fewer
+    stages mean fewer shared-memory exchanges and barriers;
+  * b threads per column (a thread owns one butterfly of radix a and
+    ceil(a / b) of radix b), or a threads ("wide": one butterfly of radix b;
+    b of the a threads take one of radix a, so no thread holds more than a
+    values) for the lengths in WIDE, where timing every table entry both ways
+    (pass 1 and 2 over L x L complex elements, 256 MiB batches) showed the
+    wide form at least 3% faster: mostly radices within a factor of 1.5 of
+    each other; the narrow form stays ahead where a is much larger than b or,
+    in complex128, a >= 35;
+  * tiles of 16 columns (complex64) / 8 (complex128) below L = 500, else 8 / 4;
+  * resident CTAs per SM asked of the register allocation (MINB): as many as
+    keep an estimate of the registers a thread needs (its largest stage's
+    values at two registers each, or four with a 1.3 margin for complex128,
+    plus 40), fit 1024 threads and 200 KB of shared memory per SM, at most 8.
+"""
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PARTS = 8
+
+
+def smooth7(n):
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def radix_ok(r):
+    return r >= 2 and smooth7(r) and (r <= 49 or (r & (r - 1) == 0 and r <= 64))
+
+
+def schedule(L):
+    best = None
+    for b in range(2, int(L ** 0.5) + 1):
+        if L % b == 0 and radix_ok(b) and radix_ok(L // b):
+            a = L // b
+            if best is None or a < best[0]:
+                best = (a, b)
+    if best is None:
+        raise ValueError(f"no two-stage schedule for {L}")
+    return best
+
+
+# Lengths whose two radices do not divide and that run faster with a threads
+# per column, per element size (bytes).
+WIDE = {
+    8: {56, 72, 90, 108, 120, 168, 180, 192, 210, 224, 240, 270, 288, 360, 378, 420, 480, 500, 504, 525, 567,
+        588, 600, 630, 648, 672, 675, 700, 720, 750, 756, 800, 810, 840, 864, 875, 896, 945, 960, 972, 980, 1008},
+    16: {48, 54, 56, 63, 72, 80, 90, 108, 120, 126, 135, 140, 150, 160, 168, 180, 210, 224, 240, 252, 270, 280,
+         288, 300, 315, 320, 336, 360, 378, 420, 432, 450, 480, 486, 500, 504, 525, 540, 560, 567, 588, 600, 630,
+         640, 648, 672, 675, 700, 720, 750, 756, 768, 800, 810, 840, 864, 896, 960},
+}
+
+
+def threads(L, sched, wide):
+    """Threads per column: L / max radix, or L / min radix (wide)."""
+    return L // (min(sched) if wide else max(sched))
+
+
+def vmax(L, sched, T):
+    return max(-(-(L // r) // T) * r for r in sched)
+
+
+def minb(L, sched, nc, es, T):
+    tpb = T * nc
+    tpbw = -(-tpb // 32) * 32
+    per = 2 * (es // 8)  # registers per complex value
+    regs = int(per * vmax(L, sched, T) * (1.0 if es == 8 else 1.3)) + 40
+    pitch = nc + 1 if nc >= 16 else nc
+    smem = max(L * pitch, nc * (L | 1)) * es
+    k = 1
+    while (k < 8 and 65536 // ((k + 1) * tpbw) >= regs and (k + 1) * tpb <= 1024
+           and (k + 1) * smem <= 200 * 1024):
+        k += 1
+    return k
+
+
+def plan(L, es):
+    """(radices, tile width, MINB, threads per column or 0) of one pass."""
+    sched = schedule(L)
+    nc = (16 if L < 500 else 8) if es == 8 else (8 if L < 500 else 4)
+    wide = sched[0] % sched[1] != 0 and L in WIDE[es]
+    T = threads(L, sched, wide)
+    return sched, nc, minb(L, sched, nc, es, T), T if wide else 0
+
+
+def cfg(L, es):
+    sched, nc, mb, tt = plan(L, es)
+    s = ", ".join(str(r) for r in sched)
+    return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
+
+
+def main(out=HERE):
+    lengths = [L for L in range(48, 1025) if smooth7(L)]
+    parts = [[] for _ in range(PARTS)]
+    for i, L in enumerate(lengths):
+        f = cfg(L, 8)
+        d = cfg(L, 16)
+        parts[i % PARTS].append(f"  v.push_back(mix_entry<{f},\n                         {f},\n"
+                                f"                         {d},\n                         {d}>());  // {L}\n")
+    for k, body in enumerate(parts):
+        with open(os.path.join(out, f"kernels_mixcols_t{k}.cu"), "w") as fh:
+            fh.write("// Generated by gen_mixcols.py; do not edit.\n"
+                     "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
+                     f"void mix_part_{k}(std::vector<MixEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
+    print(len(lengths), "lengths")
+
+
+if __name__ == "__main__":
+    main()

@@ -442,6 +442,11 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     if (s == GFFT_OK && c->gn1 == l1) return s;
     core_free(c);
   }
+  if (std::sscanf(tok.c_str(), "gpu-sm100-mixc-%lldx%lld", &l1, &l2) == 2 && l1 * l2 == n && is_smooth7(n)) {
+    gfft_status s = init_gen_twopass(c, true);
+    if (s == GFFT_OK && c->gn1 == l1) return s;
+    core_free(c);
+  }
   if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1 && ln == n && n >= 2) return init_bluestein(c);
   if (std::sscanf(tok.c_str(), "gpu-sm100-tc16-n%lld", &ln) == 1 && ln == n) return init_tc(c);
   set_error("unknown or uncompiled variant '" + tok + "' for length " + std::to_string(n));
@@ -537,6 +542,9 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
   // KernelBluestein, goes through Bluestein (planner.go:50-55).
   if (strategy != GFFT_KERNEL_BLUESTEIN && is_smooth7(n)) {
     gfft_status s = init_generic(c);
+    if (s == GFFT_OK) return s;
+    core_free(c);
+    s = init_gen_twopass(c, true);
     if (s == GFFT_OK) return s;
     core_free(c);
     s = init_gen_twopass(c);

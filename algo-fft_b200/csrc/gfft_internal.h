@@ -84,6 +84,7 @@ struct PlanCore {
   // runtime-schedule (7-smooth) plans
   GenSched gs{}, gs1{}, gs2{};
   int64_t gn1 = 0, gn2 = 0;
+  bool mixc = false;  // two passes on the compiled mixed-radix column tiles
   // Bluestein: chirps and filters per direction, sub-plan of length bm
   PlanCore* sub = nullptr;
   int64_t bm = 0;
@@ -98,7 +99,19 @@ bool make_gen_sched(int64_t n, GenSched* s);
 gfft_status init_generic(PlanCore* c);
 // Variant tokens of the runtime-radix schedules that can serve n.
 std::vector<std::string> mixed_tokens(int prec, int64_t n);
-gfft_status init_gen_twopass(PlanCore* c);
+// mixc: split n into two lengths with compiled mixed-radix column tiles
+// (mix_split) instead of the runtime-radix column kernel.
+gfft_status init_gen_twopass(PlanCore* c, bool mixc = false);
+// N1 of a split n = N1 x N2 whose factors both have compiled mixed-radix
+// column tiles, N1 <= N2 and nearest sqrt n; 0 when there is none.
+int64_t mix_split(int64_t n);
+// Compiled mixed-radix column tiles (kernels_mixcols.cu): pass 1 / pass 2
+// of the four-step over columns of length L (MIX_PASS1 / MIX_PASS2), or a
+// column batch (pass 2).  cudaErrorNotSupported for other lengths.
+struct MixColsParams;
+bool mix_cols_supported(int64_t L);
+std::vector<int64_t> mix_cols_lengths();
+cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams p, int64_t count, cudaStream_t st);
 gfft_status init_bluestein(PlanCore* c);
 // Tensor-core split-fp16 radix-16 form (complex64, powers of two 16 <= n <= 2^24;
 // n = r * 16^s with r = 2, 4, 8 takes one leading FP32 radix-r stage).

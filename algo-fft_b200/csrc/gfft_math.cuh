@@ -34,6 +34,23 @@ template <int DIR, typename C> __device__ __forceinline__ C mul_di(C a) {
   else return C{a.y, -a.x};
 }
 
+// cos / sin(2π m / R) from the generated tables (R | 64, or a 7-smooth
+// radix up to 64).
+template <int R> __host__ __device__ constexpr double root_cos(int m) {
+  if constexpr (64 % R == 0) return kCos64[m * (64 / R)];
+  else {
+    static_assert(has_root_tab(R), "no constant table for this radix");
+    return root_cos_tab(R, m);
+  }
+}
+template <int R> __host__ __device__ constexpr double root_sin(int m) {
+  if constexpr (64 % R == 0) return kSin64[m * (64 / R)];
+  else {
+    static_assert(has_root_tab(R), "no constant table for this radix");
+    return root_sin_tab(R, m);
+  }
+}
+
 // a * exp(DIR * 2πi * M / R) for a compile-time root; the quarter-turn
 // cases are exact sign swaps.
 template <int R, int M, int DIR, typename C> __device__ __forceinline__ C twc(C a) {
@@ -43,24 +60,26 @@ template <int R, int M, int DIR, typename C> __device__ __forceinline__ C twc(C 
   else if constexpr (2 * m == R) return C{-a.x, -a.y};
   else if constexpr (4 * m == R) return mul_di<DIR>(a);
   else if constexpr (4 * m == 3 * R) return mul_di<-DIR>(a);
-  else if constexpr (R == 9) {
-    constexpr double c = kCos9[m];
-    constexpr double s = DIR * kSin9[m];
-    return C{Re(c) * a.x - Re(s) * a.y, Re(c) * a.y + Re(s) * a.x};
-  } else {
-    static_assert(64 % R == 0, "constant roots cover R | 64 and R = 9");
-    constexpr double c = kCos64[m * (64 / R)];
-    constexpr double s = DIR * kSin64[m * (64 / R)];
+  else {
+    constexpr double c = root_cos<R>(m);
+    constexpr double s = DIR * root_sin<R>(m);
     return C{Re(c) * a.x - Re(s) * a.y, Re(c) * a.y + Re(s) * a.x};
   }
 }
 
-template <int R> __host__ __device__ constexpr double cos_r(int m) {
-  return R == 3 ? kCos3[m] : R == 5 ? kCos5[m] : kCos7[m];
+// First factor R1 of a composite radix R = R1 * R2 in the in-register DFT:
+// 2 for 8, 4 for the other multiples of 4 (radix-4 butterflies need no
+// multiplies), else the smallest prime factor.
+__host__ __device__ constexpr int dft_split(int R) {
+  if (R == 8) return 2;
+  if (R % 4 == 0) return 4;
+  for (int p = 2; p < R; ++p)
+    if (R % p == 0) return p;
+  return R;
 }
-template <int R> __host__ __device__ constexpr double sin_r(int m) {
-  return R == 3 ? kSin3[m] : R == 5 ? kSin5[m] : kSin7[m];
-}
+
+template <int R> __host__ __device__ constexpr double cos_r(int m) { return root_cos<R>(m); }
+template <int R> __host__ __device__ constexpr double sin_r(int m) { return root_sin<R>(m); }
 
 // Odd prime radix (3, 5, 7): pairs s_j = v_j + v_{R-j}, d_j = v_j - v_{R-j};
 // X_k = v0 + sum_j cos(2*pi*j*k/R) s_j  +-  DIR*i sum_j sin(2*pi*j*k/R) d_j.
@@ -117,9 +136,10 @@ __device__ __forceinline__ void twiddle_block(C* a) {
   }
 }
 
-// In-register DFT of R points, natural order in and out.  Powers of two and
-// 9 are split R = R1 * R2 (n = R2 n1 + n2, k = k1 + R1 k2): R2 DFTs of size
-// R1, constant twiddles W_R^{n2 k1}, R1 DFTs of size R2.
+// In-register DFT of R points, natural order in and out.  Composite R
+// (powers of two up to 64, and 7-smooth products with a constant table) is
+// split R = R1 * R2 (n = R2 n1 + n2, k = k1 + R1 k2): R2 DFTs of size R1,
+// constant twiddles W_R^{n2 k1}, R1 DFTs of size R2.
 template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) {
   if constexpr (R == 1) {
   } else if constexpr (R == 2) {
@@ -136,9 +156,9 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C* v) 
   } else if constexpr (R == 3 || R == 5 || R == 7) {
     dft_odd<R, DIR>(v);
   } else {
-    static_assert(R == 8 || R == 9 || R == 16 || R == 32 || R == 64, "unsupported radix");
-    constexpr int R1 = (R == 8) ? 2 : (R == 9) ? 3 : 4;
+    constexpr int R1 = dft_split(R);
     constexpr int R2 = R / R1;
+    static_assert(R1 > 1 && R2 > 1 && R <= 64, "unsupported radix");
     C a[R];
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2) {

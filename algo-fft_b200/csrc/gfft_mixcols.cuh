@@ -1,0 +1,257 @@
+// Compile-time mixed-radix column tiles for 7-smooth column lengths.
+//
+// The runtime-radix column kernel (k_gen_cols) pays for its generality in
+// instructions: a radix switch per stage, a runtime quotient and padded
+// address per butterfly, and two extra shared-memory passes to load and
+// store the tile.  For the column lengths the four-step splits of common
+// 7-smooth sizes produce (147 x 343 = 50421, 250 x 400 = 100000,
+// 1000 x 1000 = 10^6, ...) this header generates the same column FFTs with
+// the radices fixed at compile time, in the register/shared-memory form of
+// the power-of-two column tiles (col_stage): the first stage reads its
+// butterflies straight from HBM (runs of NC contiguous elements), the last
+// writes them straight back (pass 2) or, times the four-step twiddle,
+// transposed into shared memory for stores of whole rows (pass 1), and only
+// the exchanges between stages go through shared memory.
+//
+// A column of L = R_0 * R_1 * ... points is owned by T threads, L / max(R)
+// by default (or L / min(R) for two-stage schedules whose larger radix is
+// not a multiple of the smaller: every thread then holds at most max(R)
+// values).  Stage s (radix R_s, prefix product P_s) is Stockham's
+// self-sorting step:
+// butterfly i < L / R_s reads rows i + r L/R_s, multiplies by W_L^{r k L/(P_s R_s)}
+// (k = i mod P_s), runs DFT_{R_s} in registers and writes rows
+// (i - k) R_s + k + r P_s.  A thread takes butterflies t, t + T, ...; the
+// stages of the largest radix give every thread exactly one, smaller radices
+// several (the last partial round masked).
+//
+// Replaces, for these lengths, the reference's mixed-radix recursion
+// (internal/fft/mixedradix.go:45-188) inside the four-step of large
+// 7-smooth lengths (internal/kernels/sixstep.go:29-91).
+#pragma once
+#include "gfft_math.cuh"
+
+namespace gfft {
+
+// Stage radices R..., in the order the stages run.
+template <int... R>
+struct MixSched {
+  static constexpr int NS = sizeof...(R);
+  static constexpr int L = (1 * ... * R);
+  __host__ __device__ static constexpr int radix(int s) {
+    constexpr int a[] = {R...};
+    return a[s];
+  }
+  __host__ __device__ static constexpr int prefix(int s) {
+    int p = 1;
+    for (int i = 0; i < s; ++i) p *= radix(i);
+    return p;
+  }
+  __host__ __device__ static constexpr int rmax() {
+    int m = 1;
+    for (int i = 0; i < NS; ++i) m = radix(i) > m ? radix(i) : m;
+    return m;
+  }
+};
+
+// Tile of NC adjacent columns (NC a power of two) of length SC::L, TT
+// threads per column (0: L / max radix).
+// Shared memory: element (row, c) at row * PITCH + c, PITCH = NC + 1 (odd)
+// for NC >= 16, else rows of NC with the column XOR-swizzled by the row.
+// Pass 1's transposed result: column c at c * LP, LP = L rounded up to odd,
+// so the NC columns a warp writes at once fall in distinct banks.
+template <typename SC, int NC, int TT = 0>
+struct MixTile {
+  static_assert((NC & (NC - 1)) == 0, "NC must be a power of two");
+  static constexpr int L = SC::L;
+  static constexpr int T = TT > 0 ? TT : L / SC::rmax();  // threads per column
+  static constexpr int TPB = T * NC;
+  static_assert(TPB <= 1024, "tile needs more than 1024 threads");
+  static constexpr bool PITCHED = NC >= 16;
+  static constexpr int PITCH = PITCHED ? NC + 1 : NC;
+  static constexpr int LP = L | 1;
+  static constexpr int ELEMS1 = L * PITCH > NC * LP ? L * PITCH : NC * LP;  // pass 1
+  static constexpr int ELEMS2 = L * PITCH;                                  // pass 2
+  __host__ __device__ static constexpr int q_at(int s) { return (L / SC::radix(s) + T - 1) / T; }
+  __host__ __device__ static constexpr int vmax() {
+    int m = 1;
+    for (int s = 0; s < SC::NS; ++s) m = q_at(s) * SC::radix(s) > m ? q_at(s) * SC::radix(s) : m;
+    return m;
+  }
+  __device__ static __forceinline__ int phys(int row, int c) {
+    if constexpr (PITCHED) return row * PITCH + c;
+    else return row * NC + (c ^ (row & (NC - 1)));
+  }
+};
+
+enum { MIX_PASS1 = 1, MIX_PASS2 = 2 };
+
+// One stage of a column tile, then the next (compile-time recursion).
+//   MIX_PASS1: the first stage streams rows `ip` elements apart; the last
+//     multiplies output row k1 of column n2 by W_N^{n2 k1} and writes it to
+//     sh[c * LP + k1] (the caller stores whole rows of L).
+//   MIX_PASS2: the first stage reads rows `ip` apart through L2 (the
+//     four-step intermediate, or a caller's column batch); the last writes
+//     row k to out[k * op] scaled by `scale` for the inverse.
+template <typename C, typename SC, typename TL, int DIR, int S, int PASS>
+__device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int t, int c, bool active,
+                                          const C* __restrict__ tw, typename RealOf<C>::type scale,
+                                          const BigTwiddle& bt, int64_t n2, int64_t ip, int64_t op) {
+  constexpr int L = SC::L, T = TL::T;
+  constexpr int RS = SC::radix(S);
+  constexpr int P = SC::prefix(S);
+  constexpr int NB = L / RS;          // butterflies of the stage
+  constexpr int Q = (NB + T - 1) / T;  // per thread
+  constexpr bool GUARD = NB % T != 0;
+  constexpr bool FIRST = S == 0;
+  constexpr bool LAST = S == SC::NS - 1;
+
+  // Pass 1's four-step twiddles of the last stage, fetched before its loads
+  // so their latency hides behind them: W_N^{n2 (i + r P)} = b * s^r with
+  // b = W_N^{n2 i} (one lookup per butterfly) and s = W_N^{n2 P}.
+  [[maybe_unused]] C tw_s{}, tw_b[Q];
+  if constexpr (LAST && PASS == MIX_PASS1) {
+    if (active) {
+      tw_s = big_twiddle<C, DIR>(bt, n2 * P);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int i = t + q * T;
+        tw_b[q] = big_twiddle<C, DIR>(bt, n2 * int64_t(GUARD && i >= NB ? 0 : i));
+      }
+    }
+  }
+
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int i = t + q * T;
+      if (GUARD && i >= NB) break;
+#pragma unroll
+      for (int r = 0; r < RS; ++r) {
+        const int row = i + r * NB;
+        if constexpr (FIRST) {
+          const C* p = in + int64_t(row) * ip + c;
+          v[q * RS + r] = PASS == MIX_PASS1 ? ld_stream(p) : __ldcg(p);
+        } else {
+          v[q * RS + r] = sh[TL::phys(row, c)];
+        }
+      }
+      if constexpr (P > 1) apply_twiddles<RS, DIR>(v + q * RS, __ldg(tw + (i % P) * (L / (P * RS))));
+      dft<RS, DIR>(v + q * RS);
+    }
+  }
+
+  if constexpr (LAST && PASS == MIX_PASS2) {
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int i = t + q * T;
+        if (GUARD && i >= NB) break;
+#pragma unroll
+        for (int r = 0; r < RS; ++r) {
+          C o = v[q * RS + r];
+          if constexpr (DIR > 0) o = cscale(o, scale);
+          st_stream(out + int64_t(i + r * P) * op + c, o);
+        }
+      }
+    }
+  } else if constexpr (LAST) {
+    if constexpr (!FIRST) __syncthreads();
+    if (active) {
+      // s^r = s^(r mod 8) (s^8)^(r / 8): eight low powers and RS / 8 high
+      // ones from product trees, so a large last radix keeps few powers live
+      constexpr int NL = RS < 8 ? RS : 8, NH = (RS + 7) / 8;
+      C lo[NL], hi[NH];
+      lo[0] = C{1, 0};
+      if constexpr (NL > 1) lo[1] = tw_s;
+#pragma unroll
+      for (int r = 2; r < NL; ++r) lo[r] = cmul(lo[r / 2], lo[r - r / 2]);
+      hi[0] = C{1, 0};
+      if constexpr (NH > 1) hi[1] = cmul(lo[4], lo[4]);
+#pragma unroll
+      for (int h = 2; h < NH; ++h) hi[h] = cmul(hi[h / 2], hi[h - h / 2]);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int i = t + q * T;
+        if (GUARD && i >= NB) break;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          const C bh = h == 0 ? tw_b[q] : cmul(tw_b[q], hi[h]);
+#pragma unroll
+          for (int a = 0; a < NL && h * 8 + a < RS; ++a) {
+            const int r = h * 8 + a;
+            const C w = a == 0 ? bh : cmul(bh, lo[a]);
+            sh[c * TL::LP + i + r * P] = cmul(v[q * RS + r], w);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  } else {
+    if constexpr (!FIRST) __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int i = t + q * T;
+        if (GUARD && i >= NB) break;
+        const int k = i % P;
+        const int j = (i - k) * RS + k;
+#pragma unroll
+        for (int r = 0; r < RS; ++r) sh[TL::phys(j + r * P, c)] = v[q * RS + r];
+      }
+    }
+    __syncthreads();
+    mix_stage<C, SC, TL, DIR, S + 1, PASS>(v, in, out, sh, t, c, active, tw, scale, bt, n2, ip, op);
+  }
+}
+
+struct MixColsParams {
+  const void* src;
+  void* dst;
+  int64_t ncols;     // columns of each array (N2 in pass 1, N1 in pass 2)
+  int64_t pitch;     // input row pitch (elements)
+  int64_t opitch;    // pass 2: output row pitch
+  int64_t in_dist;   // elements between arrays of the input
+  int64_t out_dist;  // ... of the output
+  int64_t tiles;     // column tiles per array
+  const void* tw;    // W_L^m, m < L
+  BigTwiddle bt;     // pass 1: W_N^m
+  double scale;      // pass 2: 1/N for the inverse
+};
+
+// One CTA per tile of NC columns of one array (blockIdx = array * tiles + tile);
+// MINB resident CTAs per SM asked of the register allocation.
+//   MIX_PASS1: array b of x (N1 rows of N2), columns n2 in [col0, col0 + NC):
+//     column FFTs of length N1 = L, times W_N^{n2 k1}, stored as rows n2 of
+//     the scratch (N2 rows of N1 = L).
+//   MIX_PASS2: columns of L rows `pitch` apart, stored in place of their
+//     natural order `opitch` apart.
+template <typename C, typename SC, int NC, int DIR, int PASS, int MINB = 1, int TT = 0>
+__global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_cols(MixColsParams p) {
+  using TL = MixTile<SC, NC, TT>;
+  using Re = typename RealOf<C>::type;
+  constexpr int L = SC::L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw);
+  const int64_t b = blockIdx.x / p.tiles;
+  const int64_t col0 = (blockIdx.x % p.tiles) * NC;
+  const int c = threadIdx.x % NC, t = threadIdx.x / NC;
+  const bool active = col0 + c < p.ncols;
+  const C* in = static_cast<const C*>(p.src) + b * p.in_dist + col0;
+  const C* tw = static_cast<const C*>(p.tw);
+  C v[TL::vmax()];
+  if constexpr (PASS == MIX_PASS1) {
+    mix_stage<C, SC, TL, DIR, 0, MIX_PASS1>(v, in, nullptr, sh, t, c, active, tw, Re(1), p.bt, col0 + c, p.pitch, 0);
+    C* y = static_cast<C*>(p.dst) + b * p.out_dist + col0 * L;
+    const int nv = int(p.ncols - col0 < NC ? p.ncols - col0 : NC);
+    for (int e = threadIdx.x; e < L * nv; e += TL::TPB) {
+      const int cc = e / L, row = e - cc * L;
+      __stcg(y + e, sh[cc * TL::LP + row]);
+    }
+  } else {
+    C* out = static_cast<C*>(p.dst) + b * p.out_dist + col0;
+    mix_stage<C, SC, TL, DIR, 0, MIX_PASS2>(v, in, out, sh, t, c, active, tw, Re(p.scale), p.bt, 0, p.pitch,
+                                            p.opitch);
+  }
+}
+
+}  // namespace gfft

@@ -7,6 +7,7 @@
 #include <vector>
 #include "gfft_generic.cuh"
 #include "gfft_internal.h"
+#include "gfft_mixcols.cuh"
 
 namespace gfft {
 
@@ -215,6 +216,13 @@ static int64_t gen_split(int64_t n) {
   return n1;
 }
 
+int64_t mix_split(int64_t n) {
+  int64_t best = 0;
+  for (int64_t d : mix_cols_lengths())
+    if (n % d == 0 && d * d <= n && mix_cols_supported(n / d) && d > best) best = d;
+  return best;
+}
+
 std::vector<std::string> mixed_tokens(int prec, int64_t n) {
   std::vector<std::string> v;
   const size_t es = elem_bytes(prec);
@@ -224,17 +232,21 @@ std::vector<std::string> mixed_tokens(int prec, int64_t n) {
   const int want = prec == kC64 ? 16 : 8;
   if (n1 >= 2 && make_col_sched(n1, es, want, &s1) && make_col_sched(n2, es, want, &s2))
     v.push_back("gpu-sm100-mixed2-" + std::to_string(n1) + "x" + std::to_string(n2));
+  const int64_t m1 = mix_split(n);
+  if (m1 >= 2) v.push_back("gpu-sm100-mixc-" + std::to_string(m1) + "x" + std::to_string(n / m1));
   return v;
 }
 
-gfft_status init_gen_twopass(PlanCore* c) {
+gfft_status init_gen_twopass(PlanCore* c, bool mixc) {
   const int64_t n = c->n;
   const size_t es = elem_bytes(c->prec);
-  const int64_t n1 = gen_split(n);
-  const int64_t n2 = n / n1;
+  const int64_t n1 = mixc ? mix_split(n) : gen_split(n);
   if (n1 < 2) return GFFT_ERR_NOT_IMPLEMENTED;
+  const int64_t n2 = n / n1;
   const int want = c->prec == kC64 ? 16 : 8;
-  if (!make_col_sched(n1, es, want, &c->gs1) || !make_col_sched(n2, es, want, &c->gs2)) return GFFT_ERR_NOT_IMPLEMENTED;
+  if (!mixc && (!make_col_sched(n1, es, want, &c->gs1) || !make_col_sched(n2, es, want, &c->gs2)))
+    return GFFT_ERR_NOT_IMPLEMENTED;
+  c->mixc = mixc;
   GFFT_CUDA(prepare_generic_kernels());
   int shift = 0;
   while ((int64_t(1) << (2 * shift)) < n) ++shift;
@@ -255,8 +267,19 @@ gfft_status init_gen_twopass(PlanCore* c) {
   c->bt_hi = base + (n1 + n2 + nlo) * es;
   c->bt_shift = shift;
   c->algo = Algo::GenTwoPass;
-  c->name = "gpu-sm100-mixed2-" + std::to_string(n1) + "x" + std::to_string(n2);
+  c->name = std::string(mixc ? "gpu-sm100-mixc-" : "gpu-sm100-mixed2-") + std::to_string(n1) + "x" + std::to_string(n2);
   return GFFT_OK;
+}
+
+// The two passes of a mixc plan over transforms [0, m) of in / out.
+static cudaError_t mixc_passes(const PlanCore* c, int dir, const void* in, void* scratch, void* out, int64_t m,
+                               int64_t idist, int64_t odist, BigTwiddle bt, double scale, cudaStream_t st) {
+  const int64_t n = c->n;
+  MixColsParams p1{in, scratch, c->gn2, c->gn2, 0, idist, n, 0, c->tw1, bt, 1.0};
+  cudaError_t e = exec_mix_cols(c->prec, dir, MIX_PASS1, c->gn1, p1, m, st);
+  if (e != cudaSuccess) return e;
+  MixColsParams p2{scratch, out, c->gn1, c->gn1, c->gn1, n, odist, 0, c->tw2, bt, scale};
+  return exec_mix_cols(c->prec, dir, MIX_PASS2, c->gn2, p2, m, st);
 }
 
 static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
@@ -273,7 +296,9 @@ static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const
     const int64_t m = std::min(chunk, count - b0);
     const char* in = static_cast<const char*>(src) + size_t(b0) * size_t(idist) * es;
     char* out = static_cast<char*>(dst) + size_t(b0) * size_t(odist) * es;
-    if (c->prec == kC64) {
+    if (c->mixc) {
+      e = mixc_passes(c, dir, in, scratch, out, m, idist, odist, bt, scale, st);
+    } else if (c->prec == kC64) {
       e = launch_cols<float2, GEN_PASS1>(c->gs1, dir, in, scratch, m, idist, n, c->gn2, c->tw1, bt, 1.0, st);
       if (e == cudaSuccess)
         e = launch_cols<float2, GEN_PASS2>(c->gs2, dir, scratch, out, m, n, odist, c->gn1, c->tw2, bt, scale, st);
@@ -284,7 +309,7 @@ static gfft_status exec_gen_twopass(const PlanCore* c, int dir, void* dst, const
     }
   }
   cudaFreeAsync(scratch, st);
-  if (e != cudaSuccess) return cuda_status(e, "k_gen_cols");
+  if (e != cudaSuccess) return cuda_status(e, c->mixc ? "k_mix_cols" : "k_gen_cols");
   return GFFT_OK;
 }
 
@@ -303,6 +328,12 @@ gfft_status exec_columns(const GenSched& s, int prec, int dir, void* dst, const 
   }
   BigTwiddle bt{nullptr, nullptr, 0};
   const double scale = 1.0 / double(s.n);
+  if (mix_cols_supported(s.n)) {
+    const MixColsParams p{src, dst, ncols, pitch, pitch, dist, dist, 0, tw_n, bt, scale};
+    const cudaError_t e = exec_mix_cols(prec, dir, MIX_PASS2, s.n, p, count, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_mix_cols");
+    return GFFT_OK;
+  }
   cudaError_t e = prec == kC64
                       ? launch_cols<float2, GEN_PASS2>(s, dir, src, dst, count, dist, dist, ncols, tw_n, bt, scale, st, pitch)
                       : launch_cols<double2, GEN_PASS2>(s, dir, src, dst, count, dist, dist, ncols, tw_n, bt, scale, st, pitch);

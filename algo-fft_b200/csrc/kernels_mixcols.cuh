@@ -1,0 +1,68 @@
+// Launchers and table entries of the compiled mixed-radix column tiles
+// (gfft_mixcols.cuh).  The generated kernels_mixcols_t*.cu files each
+// instantiate a share of the table (gen_mixcols.py picks the schedules);
+// kernels_mixcols.cu gathers them.
+#pragma once
+#include "gfft_internal.h"
+#include "gfft_mixcols.cuh"
+
+namespace gfft {
+
+using MixFn = cudaError_t (*)(const MixColsParams&, int64_t, cudaStream_t);
+
+struct MixEntry {
+  int L;
+  int nc[2];          // tile width of pass 1 per precision (pass 2 takes the same)
+  int nc2[2];         // tile width of pass 2 per precision
+  MixFn fn[2][2][2];  // [prec][dir < 0 ? 0 : 1][pass - 1]
+};
+
+// One pass: schedule SC, NC columns per tile, MINB resident CTAs per SM,
+// TT threads per column (0: L / max radix).
+template <typename SC, int NC, int MINB, int TT = 0>
+struct MixCfg {
+  using Sched = SC;
+  static constexpr int nc = NC, minb = MINB, tt = TT;
+};
+
+template <typename C, typename CFG, int DIR, int PASS>
+cudaError_t launch_mix(const MixColsParams& p, int64_t count, cudaStream_t st) {
+  using SC = typename CFG::Sched;
+  constexpr int NC = CFG::nc;
+  using TL = MixTile<SC, NC, CFG::tt>;
+  constexpr int smem = (PASS == MIX_PASS1 ? TL::ELEMS1 : TL::ELEMS2) * int(sizeof(C));
+  auto kern = &k_mix_cols<C, SC, NC, DIR, PASS, CFG::minb, CFG::tt>;
+  static const cudaError_t attr =
+      smem > 48 * 1024 ? cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) : cudaSuccess;
+  if (attr != cudaSuccess) return attr;
+  const int64_t blocks = p.tiles * count;
+  if (blocks <= 0) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  kern<<<unsigned(blocks), TL::TPB, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+// Table entry of length L from the four pass configurations
+// (complex64 pass 1 / pass 2, complex128 pass 1 / pass 2).
+template <typename F1, typename F2, typename D1, typename D2>
+MixEntry mix_entry() {
+  static_assert(F1::Sched::L == F2::Sched::L && F1::Sched::L == D1::Sched::L && F1::Sched::L == D2::Sched::L,
+                "one length per entry");
+  MixEntry e{};
+  e.L = F1::Sched::L;
+  e.nc[kC64] = F1::nc;
+  e.nc2[kC64] = F2::nc;
+  e.nc[kC128] = D1::nc;
+  e.nc2[kC128] = D2::nc;
+  e.fn[kC64][0][0] = &launch_mix<float2, F1, -1, MIX_PASS1>;
+  e.fn[kC64][0][1] = &launch_mix<float2, F2, -1, MIX_PASS2>;
+  e.fn[kC64][1][0] = &launch_mix<float2, F1, +1, MIX_PASS1>;
+  e.fn[kC64][1][1] = &launch_mix<float2, F2, +1, MIX_PASS2>;
+  e.fn[kC128][0][0] = &launch_mix<double2, D1, -1, MIX_PASS1>;
+  e.fn[kC128][0][1] = &launch_mix<double2, D2, -1, MIX_PASS2>;
+  e.fn[kC128][1][0] = &launch_mix<double2, D1, +1, MIX_PASS1>;
+  e.fn[kC128][1][1] = &launch_mix<double2, D2, +1, MIX_PASS2>;
+  return e;
+}
+
+}  // namespace gfft

@@ -544,14 +544,15 @@ def _uneven(dev, stream, iters, gen):
 
 
 def _mixed_radix(dev, stream, iters, gen):
-    """7-smooth lengths (runtime radix, one CTA or two passes), complex64,
-    512 MiB batches; GB/s of user bytes and the error of the first
-    transforms against numpy's FP64 FFT."""
+    """7-smooth lengths (runtime radix in one CTA, or two passes over
+    compiled mixed-radix or runtime-radix column tiles), complex64, 512 MiB
+    batches; GB/s of user bytes and the error of the first transforms
+    against numpy's FP64 FFT."""
     import numpy as np
     import torch
     import algofft
     out = {}
-    for n in (60, 1000, 6000, 6561, 10000, 50421, 100000):
+    for n in (60, 1000, 6000, 6561, 10000, 50421, 62500, 100000, 117649, 1000000):
         count = (1 << 29) // (8 * n)
         x = torch.randn(2 * n * count, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
         y = torch.empty_like(x)
@@ -657,7 +658,7 @@ def _convolve(dev, stream, iters, gen):
 
 
 CASES = ("pow2_cols", "uneven600", "bs_fused", "bs_tp", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
-         "gen_cols", "tp3t", "tp2", "p16384")
+         "gen_cols", "mix_cols", "tp3t", "tp2", "p16384")
 
 
 def run_case(name: str, reps: int) -> int:
@@ -726,11 +727,13 @@ def run_case(name: str, reps: int) -> int:
         p = algofft.Plan(n, variant=f"gpu-sm100-tc16-n{n}")
         close.append(p)
         fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
-    elif name in ("l2p", "tp3t", "gen_cols", "tp2", "p16384"):
+    elif name in ("l2p", "tp3t", "gen_cols", "mix_cols", "tp2", "p16384"):
         # L2-pipelined 2^20 (16 transforms, 16 MB groups), TMA three-pass 2^23 (4), runtime two-pass 50421
-        # (160), the default plan of 2^20 (split two-pass, 16), single pass 16384 (4096)
+        # (160), compiled mixed-radix two-pass 50421 (160), the default plan of 2^20 (split two-pass, 16),
+        # single pass 16384 (4096)
         n, count, tok = {"l2p": (1 << 20, 16, "-l2p-1024x1024-c8x8-e16x16-s3-g16"), "tp3t": (1 << 23, 4, "-tp3t-"),
-                         "gen_cols": (50421, 160, "-mixed2-"), "tp2": (1 << 20, 16, None),
+                         "gen_cols": (50421, 160, "-mixed2-"), "mix_cols": (50421, 160, "-mixc-"),
+                         "tp2": (1 << 20, 16, None),
                          "p16384": (16384, 4096, None)}[name]
         x = cplx(n * count)
         y = torch.empty_like(x)

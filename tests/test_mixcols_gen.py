@@ -1,0 +1,78 @@
+"""CPU checks of the compiled mixed-radix column tiles: the committed
+kernels_mixcols_t*.cu files are what gen_mixcols.py writes, every table
+entry fits its launch limits, and the Stockham index maps the tiles use
+(gfft_mixcols.cuh: butterfly i of stage s reads rows i + r L/R_s, takes
+W_L^{r k L/(P_s R_s)} with k = i mod P_s, writes rows (i - k) R_s + k + r P_s)
+reproduce numpy's FFT for every schedule in the table."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+CSRC = os.path.join(os.path.dirname(__file__), "..", "algo-fft_b200", "csrc")
+
+
+def _gen():
+    spec = importlib.util.spec_from_file_location("gen_mixcols", os.path.join(CSRC, "gen_mixcols.py"))
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    return g
+
+
+def test_generated_files_are_current(tmp_path):
+    g = _gen()
+    g.main(str(tmp_path))
+    for k in range(g.PARTS):
+        name = f"kernels_mixcols_t{k}.cu"
+        with open(os.path.join(CSRC, name)) as a, open(tmp_path / name) as b:
+            assert a.read() == b.read(), f"{name} is stale: run gen_mixcols.py"
+
+
+def test_every_length_has_a_launchable_plan():
+    g = _gen()
+    lengths = [L for L in range(48, 1025) if g.smooth7(L)]
+    assert len(lengths) == 115
+    for L in lengths:
+        for es in (8, 16):
+            sched, nc, minb, tt = g.plan(L, es)
+            assert int(np.prod(sched)) == L and len(sched) == 2
+            assert all(g.radix_ok(r) for r in sched)
+            T = tt if tt else L // max(sched)
+            assert T * nc <= 1024 and 1 <= minb <= 8
+            pitch = nc + 1 if nc >= 16 else nc
+            assert max(L * pitch, nc * (L | 1)) * es <= 200 * 1024
+
+
+def _stockham(x, sched, T):
+    """The tile's stage loop on one column, thread by thread (threads t < T,
+    butterflies t, t + T, ...)."""
+    L = x.size
+    cur = x.astype(np.complex128)
+    P = 1
+    for R in sched:
+        nb = L // R
+        out = np.empty_like(cur)
+        for t in range(T):
+            for i in range(t, nb, T):
+                k = i % P
+                v = cur[i + nb * np.arange(R)]
+                v = v * np.exp(-2j * np.pi * np.arange(R) * k * (L // (P * R)) / L)
+                v = np.fft.fft(v)
+                out[(i - k) * R + k + P * np.arange(R)] = v
+        cur = out
+        P *= R
+    return cur
+
+
+@pytest.mark.parametrize("es", [8, 16])
+def test_index_maps_match_fft(es):
+    g = _gen()
+    rng = np.random.default_rng(5)
+    for L in [L for L in range(48, 1025) if g.smooth7(L)][::3]:
+        sched, nc, minb, tt = g.plan(L, es)
+        T = tt if tt else L // max(sched)
+        x = rng.standard_normal(L) + 1j * rng.standard_normal(L)
+        got = _stockham(x, sched, T)
+        want = np.fft.fft(x)
+        assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want), (L, sched, T)
