@@ -108,9 +108,11 @@ int64_t mix_split(int64_t n);
 // Compiled mixed-radix column tiles (kernels_mixcols.cu): pass 1 / pass 2
 // of the four-step over columns of length L (MIX_PASS1 / MIX_PASS2), or a
 // column batch (pass 2).  cudaErrorNotSupported for other lengths.
+// With p.items set (item mode) `count` is the number of CTAs of the launch.
 struct MixColsParams;
 bool mix_cols_supported(int64_t L);
 std::vector<int64_t> mix_cols_lengths();
+int mix_cols_width(int prec, int pass, int64_t L);  // columns per tile (0: not compiled)
 cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams p, int64_t count, cudaStream_t st);
 gfft_status init_bluestein(PlanCore* c);
 // Tensor-core split-fp16 radix-16 form (complex64, powers of two 16 <= n <= 2^24;

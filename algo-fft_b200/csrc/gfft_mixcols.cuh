@@ -204,6 +204,18 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
   }
 }
 
+// One transform of an uneven batch on the mixed-radix four-step: n = N1 x N2,
+// both column lengths compiled.  Offsets are in elements.
+struct MixItem {
+  int64_t off;       // the transform in src and dst
+  int64_t y;         // its N2 x N1 intermediate in the scratch
+  int64_t n;
+  int64_t lo, hi;    // W_n split tables in `tab`
+  int32_t shift;     // of the split
+  int32_t first[2];  // its first CTA in the pass-1 / pass-2 launch of its column length
+  int32_t pad_;
+};
+
 struct MixColsParams {
   const void* src;
   void* dst;
@@ -212,10 +224,16 @@ struct MixColsParams {
   int64_t opitch;    // pass 2: output row pitch
   int64_t in_dist;   // elements between arrays of the input
   int64_t out_dist;  // ... of the output
-  int64_t tiles;     // column tiles per array
+  int64_t tiles;     // column tiles per array (item mode: CTAs of the launch)
   const void* tw;    // W_L^m, m < L
   BigTwiddle bt;     // pass 1: W_N^m
   double scale;      // pass 2: 1/N for the inverse
+  // Item mode (uneven batches): CTA i works on transform items[blk[i]];
+  // src / dst are the packed batch and the scratch (pass 1) or the scratch
+  // and the packed batch (pass 2), `tab` holds the items' W_n tables.
+  const MixItem* items = nullptr;
+  const int32_t* blk = nullptr;
+  const void* tab = nullptr;
 };
 
 // One CTA per tile of NC columns of one array (blockIdx = array * tiles + tile);
@@ -225,6 +243,8 @@ struct MixColsParams {
 //     the scratch (N2 rows of N1 = L).
 //   MIX_PASS2: columns of L rows `pitch` apart, stored in place of their
 //     natural order `opitch` apart.
+// In item mode every CTA takes its transform, its columns (n / L of them,
+// the row pitch) and, for pass 1, its W_n tables from its item.
 template <typename C, typename SC, int NC, int DIR, int PASS, int MINB = 1, int TT = 0>
 __global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_cols(MixColsParams p) {
   using TL = MixTile<SC, NC, TT>;
@@ -232,25 +252,43 @@ __global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_cols(Mix
   constexpr int L = SC::L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sh = reinterpret_cast<C*>(smem_raw);
-  const int64_t b = blockIdx.x / p.tiles;
-  const int64_t col0 = (blockIdx.x % p.tiles) * NC;
+  const C* src = static_cast<const C*>(p.src);
+  C* dst = static_cast<C*>(p.dst);
+  int64_t col0, ncols = p.ncols, pitch = p.pitch, opitch = p.opitch, ioff, ooff;
+  BigTwiddle bt = p.bt;
+  Re scale = Re(p.scale);
+  if (p.items) {
+    const MixItem m = p.items[p.blk[blockIdx.x]];
+    ncols = m.n / L;
+    pitch = opitch = ncols;
+    col0 = int64_t(int(blockIdx.x) - m.first[PASS - 1]) * NC;
+    ioff = PASS == MIX_PASS1 ? m.off : m.y;
+    ooff = PASS == MIX_PASS1 ? m.y : m.off;
+    const C* tab = static_cast<const C*>(p.tab);
+    bt = BigTwiddle{tab + m.lo, tab + m.hi, m.shift};
+    scale = Re(1.0 / double(m.n));
+  } else {
+    const int64_t b = blockIdx.x / p.tiles;
+    col0 = (blockIdx.x % p.tiles) * NC;
+    ioff = b * p.in_dist;
+    ooff = b * p.out_dist;
+  }
   const int c = threadIdx.x % NC, t = threadIdx.x / NC;
-  const bool active = col0 + c < p.ncols;
-  const C* in = static_cast<const C*>(p.src) + b * p.in_dist + col0;
+  const bool active = col0 + c < ncols;
+  const C* in = src + ioff + col0;
   const C* tw = static_cast<const C*>(p.tw);
   C v[TL::vmax()];
   if constexpr (PASS == MIX_PASS1) {
-    mix_stage<C, SC, TL, DIR, 0, MIX_PASS1>(v, in, nullptr, sh, t, c, active, tw, Re(1), p.bt, col0 + c, p.pitch, 0);
-    C* y = static_cast<C*>(p.dst) + b * p.out_dist + col0 * L;
-    const int nv = int(p.ncols - col0 < NC ? p.ncols - col0 : NC);
+    mix_stage<C, SC, TL, DIR, 0, MIX_PASS1>(v, in, nullptr, sh, t, c, active, tw, Re(1), bt, col0 + c, pitch, 0);
+    C* y = dst + ooff + col0 * L;
+    const int nv = int(ncols - col0 < NC ? ncols - col0 : NC);
     for (int e = threadIdx.x; e < L * nv; e += TL::TPB) {
       const int cc = e / L, row = e - cc * L;
       __stcg(y + e, sh[cc * TL::LP + row]);
     }
   } else {
-    C* out = static_cast<C*>(p.dst) + b * p.out_dist + col0;
-    mix_stage<C, SC, TL, DIR, 0, MIX_PASS2>(v, in, out, sh, t, c, active, tw, Re(p.scale), p.bt, 0, p.pitch,
-                                            p.opitch);
+    C* out = dst + ooff + col0;
+    mix_stage<C, SC, TL, DIR, 0, MIX_PASS2>(v, in, out, sh, t, c, active, tw, scale, bt, 0, pitch, opitch);
   }
 }
 

@@ -10,6 +10,10 @@
 //     per CTA-size class, fed by a device work queue;
 //   - larger power-of-two lengths: gathered into one batch per length, run
 //     through that length's batched plan, scattered back;
+//   - larger 7-smooth lengths whose four-step factors n = N1 x N2 both have
+//     compiled mixed-radix column tiles: the two passes of every such
+//     transform in one launch per distinct N1 (pass 1) and one per distinct
+//     N2 (pass 2), each CTA finding its transform through an item table;
 //   - every other larger length through Bluestein, grouped by FFT length M
 //     (NextPow2(2n-1), plan.go:865): one gather (x chirp), one batched FFT_M,
 //     one filter product, one batched inverse FFT_M, one scatter (x chirp).
@@ -23,6 +27,7 @@
 #include <new>
 #include <vector>
 #include "gfft_internal.h"
+#include "gfft_mixcols.cuh"
 #include "gfft_uneven.cuh"
 
 namespace gfft {
@@ -98,6 +103,18 @@ struct gfft_plan_uneven {
   std::vector<Graph> graphs;
   uint64_t tick = 0;
   cudaStream_t cap = nullptr;
+  // Large 7-smooth lengths on the mixed-radix four-step (item mode).
+  struct MixLaunch {
+    int64_t L;        // column length of the launch
+    int pass;         // MIX_PASS1 / MIX_PASS2
+    int64_t tw;       // W_L table offset
+    int64_t blocks;   // CTAs
+    int32_t* d_blk = nullptr;  // item of every CTA
+  };
+  std::vector<MixItem> mix_items;
+  MixItem* d_mix_items = nullptr;
+  std::vector<MixLaunch> mix_launches;  // pass-1 launches first
+  int64_t mix_scratch = 0;              // elements of the intermediates
   // Recorded after every call's work: the next call, on whatever stream,
   // waits for it, so calls on one plan never overlap on the device (they
   // share the work buffers and queue counters above).
@@ -141,6 +158,9 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
   std::map<int64_t, int64_t> chirp_off, filt_off;
   std::map<int64_t, int> big_pow2_group;          // large pow2 length -> group
   std::map<int64_t, int> big_bs_group;            // M -> group
+  std::map<int64_t, int64_t> mix_n1;              // mixed-radix four-step length -> N1
+  std::map<int64_t, int64_t> mix_lo, mix_hi;      // its W_n split tables
+  std::map<int64_t, int> mix_shift;
   int64_t cursor = 0;
   auto alloc = [&](int64_t n) {
     const int64_t at = cursor;
@@ -168,6 +188,18 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
       Group g;
       g.M = n;
       p->groups.push_back(g);
+      continue;
+    }
+    const int64_t m1 = is_smooth7(n) ? mix_split(n) : 0;
+    if (m1 >= 2) {
+      mix_n1[n] = m1;
+      for (int64_t L : {m1, n / m1})
+        if (!tw_off.count(L)) tw_off[L] = alloc(L);
+      int shift = 0;
+      while ((int64_t(1) << (2 * shift)) < n) ++shift;
+      mix_shift[n] = shift;
+      mix_lo[n] = alloc(int64_t(1) << shift);
+      mix_hi[n] = alloc((n + (int64_t(1) << shift) - 1) >> shift);
       continue;
     }
     int64_t M = 1;
@@ -202,6 +234,12 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
   char* tab = static_cast<char*>(p->tab);
   for (auto& kv : tw_off) {
     gfft_status s = fill_twiddles(p->prec, tab + kv.second * es, kv.first, kv.first, 1, 0);
+    if (s != GFFT_OK) return s;
+  }
+  for (auto& kv : mix_n1) {
+    const int64_t n = kv.first, nlo = int64_t(1) << mix_shift[n];
+    gfft_status s = fill_twiddles(p->prec, tab + mix_lo[n] * es, n, nlo, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(p->prec, tab + mix_hi[n] * es, n, (n + nlo - 1) / nlo, nlo, 0);
     if (s != GFFT_OK) return s;
   }
   for (auto& kv : chirp_off) {
@@ -244,6 +282,16 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     }
     if ((n & (n - 1)) == 0) {
       p->groups[big_pow2_group[n]].items.push_back(BigItem{p->off[i], n, 0, 0});
+    } else if (mix_n1.count(n)) {
+      MixItem m{};
+      m.off = p->off[i];
+      m.y = p->mix_scratch;
+      m.n = n;
+      m.lo = mix_lo[n];
+      m.hi = mix_hi[n];
+      m.shift = mix_shift[n];
+      p->mix_scratch += n;
+      p->mix_items.push_back(m);
     } else {
       int64_t M = 1;
       while (M < 2 * n - 1) M <<= 1;
@@ -292,6 +340,40 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     GFFT_CUDA(cudaMemcpy(g.d_items, g.items.data(), g.items.size() * sizeof(BigItem), cudaMemcpyHostToDevice));
     GFFT_CUDA(cudaMalloc(&g.work, g.items.size() * size_t(g.M) * es));
   }
+  // mixed-radix four-step items: one launch per column length and pass,
+  // each CTA one column tile of one item
+  if (!p->mix_items.empty()) {
+    for (int pass : {int(MIX_PASS1), int(MIX_PASS2)}) {
+      std::map<int64_t, std::vector<int>> by_len;
+      for (int i = 0; i < int(p->mix_items.size()); ++i) {
+        const int64_t n = p->mix_items[i].n, n1 = mix_n1[n];
+        by_len[pass == MIX_PASS1 ? n1 : n / n1].push_back(i);
+      }
+      for (auto& kv : by_len) {
+        const int64_t L = kv.first;
+        const int nc = mix_cols_width(p->prec, pass, L);
+        if (nc <= 0) return GFFT_ERR_NOT_IMPLEMENTED;
+        std::vector<int32_t> blk;
+        for (int i : kv.second) {
+          MixItem& m = p->mix_items[i];
+          m.first[pass - 1] = int32_t(blk.size());
+          const int64_t tiles = (m.n / L + nc - 1) / nc;
+          blk.insert(blk.end(), size_t(tiles), int32_t(i));
+        }
+        gfft_plan_uneven::MixLaunch ml;
+        ml.L = L;
+        ml.pass = pass;
+        ml.tw = tw_off[L];
+        ml.blocks = int64_t(blk.size());
+        GFFT_CUDA(cudaMalloc(&ml.d_blk, blk.size() * sizeof(int32_t)));
+        p->mix_launches.push_back(ml);
+        GFFT_CUDA(cudaMemcpy(ml.d_blk, blk.data(), blk.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+      }
+    }
+    GFFT_CUDA(cudaMalloc(&p->d_mix_items, p->mix_items.size() * sizeof(MixItem)));
+    GFFT_CUDA(cudaMemcpy(p->d_mix_items, p->mix_items.data(), p->mix_items.size() * sizeof(MixItem),
+                         cudaMemcpyHostToDevice));
+  }
   GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
   GFFT_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
   GFFT_CUDA(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
@@ -307,6 +389,24 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
     k_uneven<C, DIR><<<K.grid, K.cta, K.smem, st>>>(src, dst, K.d_items, int(K.items.size()), p->d_descs,
                                                     static_cast<const C*>(p->tab), p->counters + k);
     GFFT_CUDA(cudaGetLastError());
+  }
+  if (!p->mix_items.empty()) {
+    void* scratch = nullptr;
+    GFFT_CUDA(ws_alloc(&scratch, size_t(p->mix_scratch) * sizeof(C), st));
+    cudaError_t e = cudaSuccess;
+    for (const auto& ml : p->mix_launches) {
+      MixColsParams mp{};
+      mp.src = ml.pass == MIX_PASS1 ? static_cast<const void*>(src) : scratch;
+      mp.dst = ml.pass == MIX_PASS1 ? scratch : static_cast<void*>(dst);
+      mp.tw = static_cast<const C*>(p->tab) + ml.tw;
+      mp.items = p->d_mix_items;
+      mp.blk = ml.d_blk;
+      mp.tab = p->tab;
+      e = exec_mix_cols(p->prec, DIR, ml.pass, ml.L, mp, ml.blocks, st);
+      if (e != cudaSuccess) break;
+    }
+    cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_mix_cols");
   }
   for (Group& g : p->groups) {
     const int64_t rows = int64_t(g.items.size());
@@ -430,6 +530,9 @@ void gfft_plan_uneven_close(gfft_plan_uneven* p) {
     core_free(kv.second);
     delete kv.second;
   }
+  for (auto& ml : p->mix_launches)
+    if (ml.d_blk) cudaFree(ml.d_blk);
+  if (p->d_mix_items) cudaFree(p->d_mix_items);
   if (p->d_descs) cudaFree(p->d_descs);
   if (p->tab) cudaFree(p->tab);
   if (p->counters) cudaFree(p->counters);

@@ -45,11 +45,22 @@ std::vector<int64_t> mix_cols_lengths() {
   return v;
 }
 
+int mix_cols_width(int prec, int pass, int64_t L) {
+  const MixEntry* e = find(L);
+  if (!e || (prec != kC64 && prec != kC128)) return 0;
+  return pass == MIX_PASS1 ? e->nc[prec] : e->nc2[prec];
+}
+
 cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams p, int64_t count, cudaStream_t st) {
   const MixEntry* e = find(L);
   if (!e || (pass != MIX_PASS1 && pass != MIX_PASS2) || (prec != kC64 && prec != kC128)) return cudaErrorNotSupported;
-  const int nc = pass == MIX_PASS1 ? e->nc[prec] : e->nc2[prec];
-  p.tiles = (p.ncols + nc - 1) / nc;
+  if (p.items) {
+    p.tiles = count;  // item mode: `count` CTAs, each finds its transform
+    count = 1;
+  } else {
+    const int nc = pass == MIX_PASS1 ? e->nc[prec] : e->nc2[prec];
+    p.tiles = (p.ncols + nc - 1) / nc;
+  }
   return e->fn[prec][dir < 0 ? 0 : 1][pass - 1](p, count, st);
 }
 

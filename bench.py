@@ -657,7 +657,7 @@ def _convolve(dev, stream, iters, gen):
     return out
 
 
-CASES = ("pow2_cols", "uneven600", "bs_fused", "bs_tp", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
+CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
          "gen_cols", "mix_cols", "tp3t", "tp2", "p16384")
 
 
@@ -685,8 +685,8 @@ def run_case(name: str, reps: int) -> int:
         p = algofft.NewPlan(n)
         close.append(p)
         fn = lambda: p.StridedBatch(y, x, cols, cols, 1)  # noqa: E731
-    elif name == "uneven600":  # 600 transforms of the uneven workload's length mix
-        L = algofft.uneven_lengths(600, seed=1)
+    elif name in ("uneven600", "uneven20000"):  # 600 transforms of the uneven mix / the whole workload
+        L = algofft.uneven_lengths(600, seed=1) if name == "uneven600" else algofft.uneven_lengths(20000, seed=0)
         p = algofft.PlanUneven(L)
         close.append(p)
         x = cplx(p.Total())
@@ -743,7 +743,11 @@ def run_case(name: str, reps: int) -> int:
         fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
     else:
         raise SystemExit(f"unknown case {name}; cases: {', '.join(CASES)}")
+    # the calls sit in an NVTX range "case" (ncu --nvtx --nvtx-include case/
+    # captures them without the plans' setup launches)
+    torch.cuda.nvtx.range_push("case")
     ms = _median_ms(fn, torch.cuda.current_stream(dev), reps)
+    torch.cuda.nvtx.range_pop()
     for c in close:
         c.Close()
     print(json.dumps({"case": name, "reps": reps, "median_ms": ms}))

@@ -12,10 +12,14 @@ from helpers import rel_l2, seeded_complex, tol_c2c
 pytestmark = pytest.mark.gpu
 
 # every route of the plan: 1 and 2, CTA-sized 7-smooth, CTA-sized Bluestein
-# (primes), large powers of two (gathered per length), large 7-smooth and
-# large primes (Bluestein grouped by FFT length), repeats of one length
+# (primes), large powers of two (gathered per length), large 7-smooth (the
+# mixed-radix four-step, one launch per factor length: 13440 = 112 x 120,
+# 21609 = 147 x 147 and 50421 = 147 x 343 share a pass-1 launch, 25000 =
+# 125 x 200 and 40000 = 200 x 200 a pass-2 launch), large primes (Bluestein
+# grouped by FFT length), repeats of one length
 LENGTHS = [1, 2, 3, 5, 7, 8, 13, 64, 97, 360, 1009, 1024, 2048, 4099, 5003, 6000, 8191, 12289, 16384,
-           25000, 32768, 40000, 65521, 65536, 1009, 64, 65536, 360, 131072, 1 << 20]
+           25000, 32768, 40000, 65521, 65536, 1009, 64, 65536, 360, 131072, 1 << 20, 13440, 21609, 50421,
+           50421, 62500, 40000]
 
 
 def _tol(n, c128):
