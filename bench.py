@@ -729,10 +729,10 @@ def run_case(name: str, reps: int) -> int:
         fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
     elif name in ("l2p", "tp3t", "gen_cols", "mix_cols", "tp2", "p16384"):
         # L2-pipelined 2^20 (16 transforms, 16 MB groups), TMA three-pass 2^23 (4), runtime two-pass 50421
-        # (160), compiled mixed-radix two-pass 50421 (160), the default plan of 2^20 (split two-pass, 16),
+        # (160), compiled mixed-radix two-pass 50421 (640: 256 MiB), the default plan of 2^20 (split two-pass, 16),
         # single pass 16384 (4096)
         n, count, tok = {"l2p": (1 << 20, 16, "-l2p-1024x1024-c8x8-e16x16-s3-g16"), "tp3t": (1 << 23, 4, "-tp3t-"),
-                         "gen_cols": (50421, 160, "-mixed2-"), "mix_cols": (50421, 160, "-mixc-"),
+                         "gen_cols": (50421, 160, "-mixed2-"), "mix_cols": (50421, 640, "-mixc-"),
                          "tp2": (1 << 20, 16, None),
                          "p16384": (16384, 4096, None)}[name]
         x = cplx(n * count)
