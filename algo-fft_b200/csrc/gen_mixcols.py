@@ -1,6 +1,10 @@
 """Writes kernels_mixcols_t0.cu .. kernels_mixcols_t7.cu: the compiled
 mixed-radix column tiles (gfft_mixcols.cuh) of every 7-smooth column length
-48 <= L <= 1024, spread over eight files so nvcc builds them in parallel.
+48 <= L <= 1024, spread over eight files so nvcc builds them in parallel; and
+kernels_mixbs_t0.cu .. kernels_mixbs_t2.cu: the Bluestein chain's passes
+(gfft_mixbs.cuh) for the column lengths its FFT lengths M = M1 x M2 are built
+from (BS_LENGTHS: the multiples of 16 up to 512, whose products come within
+1.5% of the best 7-smooth M on average), with the same schedules.
 
 Schedule rule, from timing the candidates on a B200 (two stages against three
 and four, several tile widths and occupancies, at L = 100..1000):
@@ -25,6 +29,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PARTS = 8
+BS_PARTS = 3
 
 
 def smooth7(n):
@@ -99,6 +104,10 @@ def cfg(L, es):
     return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
 
 
+def bs_lengths():
+    return [L for L in range(48, 513) if smooth7(L) and L % 16 == 0]
+
+
 def main(out=HERE):
     lengths = [L for L in range(48, 1025) if smooth7(L)]
     parts = [[] for _ in range(PARTS)]
@@ -112,7 +121,15 @@ def main(out=HERE):
             fh.write("// Generated by gen_mixcols.py; do not edit.\n"
                      "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
                      f"void mix_part_{k}(std::vector<MixEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
-    print(len(lengths), "lengths")
+    bparts = [[] for _ in range(BS_PARTS)]
+    for i, L in enumerate(bs_lengths()):
+        bparts[i % BS_PARTS].append(f"  v.push_back(mix_bs_entry<{cfg(L, 8)},\n                            {cfg(L, 16)}>());  // {L}\n")
+    for k, body in enumerate(bparts):
+        with open(os.path.join(out, f"kernels_mixbs_t{k}.cu"), "w") as fh:
+            fh.write("// Generated by gen_mixcols.py; do not edit.\n"
+                     "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
+                     f"void mix_bs_part_{k}(std::vector<MixBsEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
+    print(len(lengths), "lengths,", len(bs_lengths()), "Bluestein lengths")
 
 
 if __name__ == "__main__":

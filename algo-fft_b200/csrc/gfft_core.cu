@@ -380,6 +380,14 @@ std::vector<std::string> variant_tokens(int prec, int64_t n) {
     // (planner.go:50-55 picks by smoothness alone)
     for (const std::string& t : mixed_tokens(prec, n)) v.push_back(t);
     v.push_back("gpu-sm100-bluestein-n" + std::to_string(n));
+  } else if (n > 1) {
+    // Bluestein: a smaller mixed FFT length (a product of compiled column
+    // lengths) against NextPow2(2n - 1)
+    int64_t m1 = 0;
+    if (bs_mixed_choice(n, &m1) > 0) {
+      v.push_back("gpu-sm100-bluestein-n" + std::to_string(n) + "-mx");
+      v.push_back("gpu-sm100-bluestein-n" + std::to_string(n) + "-p2");
+    }
   }
   return v;
 }
@@ -447,7 +455,12 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
     if (s == GFFT_OK && c->gn1 == l1) return s;
     core_free(c);
   }
-  if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1 && ln == n && n >= 2) return init_bluestein(c);
+  if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1 && ln == n && n >= 2) {
+    const std::string head = "gpu-sm100-bluestein-n" + std::to_string(n);
+    const bool mx = tok.compare(0, head.size() + 3, head + "-mx") == 0;
+    const bool p2 = tok.compare(0, head.size() + 3, head + "-p2") == 0;
+    return init_bluestein(c, mx ? kBsMixed : p2 ? kBsPow2 : kBsAuto);
+  }
   if (std::sscanf(tok.c_str(), "gpu-sm100-tc16-n%lld", &ln) == 1 && ln == n) return init_tc(c);
   set_error("unknown or uncompiled variant '" + tok + "' for length " + std::to_string(n));
   return GFFT_ERR_INVALID_ARGUMENT;
@@ -573,6 +586,8 @@ void core_free(PlanCore* c) {
     delete c->sub;
     c->sub = nullptr;
   }
+  c->mixc = false;
+  c->bsm = false;
   c->algo = Algo::Trivial;
 }
 

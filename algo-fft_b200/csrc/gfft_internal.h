@@ -85,9 +85,12 @@ struct PlanCore {
   GenSched gs{}, gs1{}, gs2{};
   int64_t gn1 = 0, gn2 = 0;
   bool mixc = false;  // two passes on the compiled mixed-radix column tiles
-  // Bluestein: chirps and filters per direction, sub-plan of length bm
+  // Bluestein: chirps and filters per direction, sub-plan of length bm;
+  // bsm: bm = gn1 x gn2 on the compiled mixed-radix tiles (tw1 = W_gn1,
+  // tw2 = W_gn2, bt_* = W_bm split)
   PlanCore* sub = nullptr;
   int64_t bm = 0;
+  bool bsm = false;
   void* bs_w[2] = {nullptr, nullptr};
   void* bs_f[2] = {nullptr, nullptr};
 };
@@ -114,7 +117,23 @@ bool mix_cols_supported(int64_t L);
 std::vector<int64_t> mix_cols_lengths();
 int mix_cols_width(int prec, int pass, int64_t L);  // columns per tile (0: not compiled)
 cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams p, int64_t count, cudaStream_t st);
-gfft_status init_bluestein(PlanCore* c);
+// Bluestein on the compiled tiles (gfft_mixbs.cuh): the smallest FFT length
+// M = M1 x M2 >= 2n - 1 its column lengths build (M1 <= M2 returned in *m1;
+// 0 when none), and one of its passes (BSK_IN / BSK_FILT / BSK_OUT) over
+// `count` transforms, or `count` CTAs in item mode.
+struct MixBsParams;
+int64_t bs_mixed_length(int64_t n, int64_t* m1);
+int mix_bs_width(int prec, int64_t L);
+cudaError_t exec_mix_bs(int prec, int kind, int64_t L, MixBsParams p, int64_t count, cudaStream_t st);
+// Bluestein's FFT length: kBsAuto takes the mixed length (a product of
+// compiled column lengths) when it is at most kBsMixedRatio of
+// NextPow2(2n - 1), the reference's; kBsPow2 / kBsMixed force either (the
+// latter where a smaller mixed length exists).  bs_mixed_choice: that
+// smaller mixed length (0: none, or the one-CTA fused range).
+enum { kBsAuto = 0, kBsPow2 = 1, kBsMixed = 2 };
+constexpr double kBsMixedRatio = 0.65;
+int64_t bs_mixed_choice(int64_t n, int64_t* m1);
+gfft_status init_bluestein(PlanCore* c, int mode = kBsAuto);
 // Tensor-core split-fp16 radix-16 form (complex64, powers of two 16 <= n <= 2^24;
 // n = r * 16^s with r = 2, 4, 8 takes one leading FP32 radix-r stage).
 bool tc_supported(int64_t n);

@@ -1,0 +1,172 @@
+// Bluestein's chain on the compiled mixed-radix column tiles, for FFT
+// lengths M = M1 x M2 that are not powers of two.
+//
+// The reference pads to M = NextPow2(2n - 1) (plan.go:865), which costs
+// 2..4 times n per FFT; any M >= 2n - 1 gives the same product up to
+// rounding.  Here M is the smallest product of two compiled column lengths
+// (multiples of 16 up to 512) that is at least 2n - 1, used when it is below
+// the power of two: about 0.76 of it on average over primes 8K..131K.  The
+// element-wise steps ride in the passes, as in the power-of-two chain
+// (kernels_bluestein_tp.cu):
+//   BSK_IN   forward pass 1 (columns of M1), its loads the chirp-weighted,
+//            zero-padded input a_m = x_m w_m (m < n), scratch out;
+//   BSK_FILT forward pass 2 (columns of M2), its stores the spectrum times
+//            the filter, Z_k = A_k F_k, in natural order back into the
+//            scratch (a tile writes exactly the addresses it read);
+//   the inverse FFT's pass 1 is the plain column tile (k_mix_cols pass 1,
+//            inverse direction), scratch to work;
+//   BSK_OUT  inverse pass 2, its stores y_k = w_k z_k / M (and 1/n for the
+//            inverse transform) for k < n only.
+// The chirp w and filter F of the forward direction serve the inverse as
+// conj(w) and conj(F[(M - k) mod M]) (flag `inv`).  Index maps are the
+// four-step's: input m = M2 n1 + n2, output k = k1 + M1 k2.
+#pragma once
+#include "gfft_mixcols.cuh"
+
+namespace gfft {
+
+enum { BSK_IN = 0, BSK_FILT = 1, BSK_OUT = 2 };
+
+// One transform of an uneven batch on this chain (offsets in elements).
+struct MixBsItem {
+  int64_t off;        // the transform in the user's input and output
+  int64_t s;          // its M-element rows in the scratch and work buffers
+  int64_t n, M;
+  int64_t chirp, filt;  // forward chirp (n) and filter spectrum (M) in `tab`
+  int64_t lo, hi;       // W_M split tables in `tab`
+  int32_t shift;
+  int32_t first[3];     // first CTA in its BSK_IN / BSK_FILT / BSK_OUT launch
+};
+
+struct MixBsParams {
+  const void* x;      // user input
+  void* y;            // user output
+  void* scratch;      // M elements per transform
+  void* work;         // M elements per transform
+  int64_t n, M, idist, odist;  // batch mode: every transform alike
+  const void* w;      // batch mode: chirp of the direction asked for
+  const void* f;      // batch mode: filter spectrum of that direction
+  const void* tw;     // W_L, L the launch's column length
+  BigTwiddle bt;      // W_M (BSK_IN)
+  int64_t tiles;      // batch mode: column tiles per transform; item mode: CTAs
+  double scale;       // batch mode: output scale (1/n for the inverse)
+  int inv;            // item mode: 1 for the inverse (conjugate tables, 1/n)
+  const MixBsItem* items = nullptr;
+  const int32_t* blk = nullptr;
+  const void* tab = nullptr;
+};
+
+template <typename C>
+__device__ __forceinline__ C bs_chirp(const C* w, int64_t m, int inv) {
+  C v = __ldg(w + m);
+  if (inv) v.y = -v.y;
+  return v;
+}
+
+template <typename C>
+struct MixBsIn {
+  static constexpr bool kLoad = true, kStore = false;
+  const C* x;
+  const C* w;
+  int64_t n, pitch, col0;
+  int inv;
+  __device__ __forceinline__ C load(int row, int c) const {
+    const int64_t m = int64_t(row) * pitch + col0 + c;
+    return m < n ? cmul(ld_stream(x + m), bs_chirp(w, m, inv)) : C{0, 0};
+  }
+};
+
+template <typename C>
+struct MixBsFilt {
+  static constexpr bool kLoad = false, kStore = true;
+  C* z;
+  const C* f;
+  int64_t m1, col0, M;
+  int inv;
+  __device__ __forceinline__ void store(int row, int c, C v) const {
+    const int64_t k = col0 + c + m1 * int64_t(row);
+    const C fk = inv ? cconj(__ldg(f + (k == 0 ? 0 : M - k))) : __ldg(f + k);
+    __stcg(z + k, cmul(v, fk));
+  }
+};
+
+template <typename C>
+struct MixBsOut {
+  static constexpr bool kLoad = false, kStore = true;
+  C* y;
+  const C* w;
+  int64_t n, m1, col0;
+  typename RealOf<C>::type scale;
+  int inv;
+  __device__ __forceinline__ void store(int row, int c, C v) const {
+    const int64_t k = col0 + c + m1 * int64_t(row);
+    if (k < n) st_stream(y + k, cscale(cmul(v, bs_chirp(w, k, inv)), scale));
+  }
+};
+
+// One CTA per column tile of one transform (batch mode: blockIdx =
+// transform * tiles + tile; item mode: items[blk[blockIdx]]).
+template <typename C, typename SC, int NC, int KIND, int MINB = 1, int TT = 0>
+__global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_bs(MixBsParams p) {
+  using TL = MixTile<SC, NC, TT>;
+  using Re = typename RealOf<C>::type;
+  constexpr int L = SC::L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw);
+  int64_t col0, off_x, off_y, s, n, M;
+  const C* w;
+  const C* f;
+  BigTwiddle bt = p.bt;
+  Re oscale;
+  if (p.items) {
+    const MixBsItem m = p.items[p.blk[blockIdx.x]];
+    col0 = int64_t(int(blockIdx.x) - m.first[KIND]) * NC;
+    off_x = off_y = m.off;
+    s = m.s;
+    n = m.n;
+    M = m.M;
+    const C* tab = static_cast<const C*>(p.tab);
+    w = tab + m.chirp;
+    f = tab + m.filt;
+    bt = BigTwiddle{tab + m.lo, tab + m.hi, m.shift};
+    oscale = Re(p.inv ? 1.0 / double(m.n) : 1.0);
+  } else {
+    const int64_t b = blockIdx.x / p.tiles;
+    col0 = (blockIdx.x % p.tiles) * NC;
+    off_x = b * p.idist;
+    off_y = b * p.odist;
+    s = b * p.M;
+    n = p.n;
+    M = p.M;
+    w = static_cast<const C*>(p.w);
+    f = static_cast<const C*>(p.f);
+    oscale = Re(p.scale);  // batch mode: the direction's own tables
+  }
+  const int64_t ncols = M / L;  // M2 for BSK_IN, M1 for the pass-2 kinds
+  const int c = threadIdx.x % NC, t = threadIdx.x / NC;
+  const bool active = col0 + c < ncols;
+  const C* tw = static_cast<const C*>(p.tw);
+  C* scratch = static_cast<C*>(p.scratch);
+  C v[TL::vmax()];
+  if constexpr (KIND == BSK_IN) {
+    const MixBsIn<C> io{static_cast<const C*>(p.x) + off_x, w, n, ncols, col0, p.inv};
+    mix_stage<C, SC, TL, -1, 0, MIX_PASS1, MixBsIn<C>>(v, nullptr, nullptr, sh, t, c, active, tw, Re(1), bt,
+                                                       col0 + c, ncols, 0, io);
+    C* yt = scratch + s + col0 * L;
+    const int nv = int(ncols - col0 < NC ? ncols - col0 : NC);
+    for (int e = threadIdx.x; e < L * nv; e += TL::TPB) {
+      const int cc = e / L, row = e - cc * L;
+      __stcg(yt + e, sh[cc * TL::LP + row]);
+    }
+  } else if constexpr (KIND == BSK_FILT) {
+    const MixBsFilt<C> io{scratch + s, f, ncols, col0, M, p.inv};
+    mix_stage<C, SC, TL, -1, 0, MIX_PASS2, MixBsFilt<C>>(v, scratch + s + col0, nullptr, sh, t, c, active, tw,
+                                                         Re(1), bt, 0, ncols, ncols, io);
+  } else {
+    const MixBsOut<C> io{static_cast<C*>(p.y) + off_y, w, n, ncols, col0, oscale, p.inv};
+    mix_stage<C, SC, TL, +1, 0, MIX_PASS2, MixBsOut<C>>(v, static_cast<const C*>(p.work) + s + col0, nullptr, sh, t,
+                                                        c, active, tw, Re(1.0 / double(M)), bt, 0, ncols, ncols, io);
+  }
+}
+
+}  // namespace gfft

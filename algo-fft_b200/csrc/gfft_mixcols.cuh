@@ -85,6 +85,13 @@ struct MixTile {
 
 enum { MIX_PASS1 = 1, MIX_PASS2 = 2 };
 
+// Hooks of mix_stage: kLoad replaces the first stage's loads by
+// io.load(row, c), kStore the last stage's pass-2 stores by
+// io.store(row, c, value) (the value already scaled for the inverse).
+struct MixNoIO {
+  static constexpr bool kLoad = false, kStore = false;
+};
+
 // One stage of a column tile, then the next (compile-time recursion).
 //   MIX_PASS1: the first stage streams rows `ip` elements apart; the last
 //     multiplies output row k1 of column n2 by W_N^{n2 k1} and writes it to
@@ -92,10 +99,11 @@ enum { MIX_PASS1 = 1, MIX_PASS2 = 2 };
 //   MIX_PASS2: the first stage reads rows `ip` apart through L2 (the
 //     four-step intermediate, or a caller's column batch); the last writes
 //     row k to out[k * op] scaled by `scale` for the inverse.
-template <typename C, typename SC, typename TL, int DIR, int S, int PASS>
+template <typename C, typename SC, typename TL, int DIR, int S, int PASS, typename IO = MixNoIO>
 __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int t, int c, bool active,
                                           const C* __restrict__ tw, typename RealOf<C>::type scale,
-                                          const BigTwiddle& bt, int64_t n2, int64_t ip, int64_t op) {
+                                          const BigTwiddle& bt, int64_t n2, int64_t ip, int64_t op,
+                                          const IO& io = IO()) {
   constexpr int L = SC::L, T = TL::T;
   constexpr int RS = SC::radix(S);
   constexpr int P = SC::prefix(S);
@@ -128,7 +136,9 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
 #pragma unroll
       for (int r = 0; r < RS; ++r) {
         const int row = i + r * NB;
-        if constexpr (FIRST) {
+        if constexpr (FIRST && IO::kLoad) {
+          v[q * RS + r] = io.load(row, c);
+        } else if constexpr (FIRST) {
           const C* p = in + int64_t(row) * ip + c;
           v[q * RS + r] = PASS == MIX_PASS1 ? ld_stream(p) : __ldcg(p);
         } else {
@@ -150,7 +160,8 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
         for (int r = 0; r < RS; ++r) {
           C o = v[q * RS + r];
           if constexpr (DIR > 0) o = cscale(o, scale);
-          st_stream(out + int64_t(i + r * P) * op + c, o);
+          if constexpr (IO::kStore) io.store(i + r * P, c, o);
+          else st_stream(out + int64_t(i + r * P) * op + c, o);
         }
       }
     }
@@ -200,7 +211,7 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
       }
     }
     __syncthreads();
-    mix_stage<C, SC, TL, DIR, S + 1, PASS>(v, in, out, sh, t, c, active, tw, scale, bt, n2, ip, op);
+    mix_stage<C, SC, TL, DIR, S + 1, PASS, IO>(v, in, out, sh, t, c, active, tw, scale, bt, n2, ip, op, io);
   }
 }
 

@@ -7,6 +7,7 @@
 #include <vector>
 #include "gfft_generic.cuh"
 #include "gfft_internal.h"
+#include "gfft_mixbs.cuh"
 #include "gfft_mixcols.cuh"
 
 namespace gfft {
@@ -373,21 +374,58 @@ __global__ void k_bs_post(C* y, const C* work, const C* w, int64_t n, int64_t M,
 
 static unsigned grid_for(int64_t total) { return unsigned(std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 32))); }
 
-gfft_status init_bluestein(PlanCore* c) {
+int64_t bs_mixed_choice(int64_t n, int64_t* m1) {
+  int64_t M = 1;
+  while (M < 2 * n - 1) M <<= 1;
+  const int64_t mx = bs_mixed_length(n, m1);
+  return M > 16384 && mx > 0 && mx < M ? mx : 0;
+}
+
+gfft_status init_bluestein(PlanCore* c, int mode) {
   const int64_t n = c->n;
   int64_t M = 1;
   while (M < 2 * n - 1) M <<= 1;  // plan.go:865 NextPowerOfTwo(2n-1)
+  // Beyond the one-CTA fused kernel, a smaller FFT length built from two
+  // compiled column lengths (the product is the same up to rounding).  Its
+  // passes move about 1.35x more time per element than the power-of-two
+  // chain's, so the automatic choice takes it only at <= 0.65 of M.
+  int64_t m1 = 0;
+  const int64_t mx = bs_mixed_choice(n, &m1);
+  const bool bsm = mx > 0 && (mode == kBsMixed || (mode == kBsAuto && double(mx) <= kBsMixedRatio * double(M)));
+  if (bsm) M = mx;
   const size_t es = elem_bytes(c->prec);
   c->sub = new PlanCore;
   gfft_status s = core_init(c->sub, c->prec, M, c->device);
   if (s != GFFT_OK) return s;
-  // [chirp fwd | chirp inv | filter fwd | filter inv]
-  GFFT_CUDA(cudaMalloc(&c->tw, size_t(2 * n + 2 * M) * es));
+  // [chirp fwd | chirp inv | filter fwd | filter inv], then for the mixed
+  // chain [W_M1 | W_M2 | W_M low | W_M high]
+  int shift = 0;
+  while ((int64_t(1) << (2 * shift)) < M) ++shift;
+  const int64_t nlo = int64_t(1) << shift, nhi = (M + nlo - 1) >> shift;
+  const int64_t m2 = bsm ? M / m1 : 0;
+  const int64_t extra = bsm ? m1 + m2 + nlo + nhi : 0;
+  GFFT_CUDA(cudaMalloc(&c->tw, size_t(2 * n + 2 * M + extra) * es));
   char* base = static_cast<char*>(c->tw);
   void* wf = base;
   void* wi = base + n * es;
   void* ff = base + 2 * n * es;
   void* fi = base + (2 * n + M) * es;
+  if (bsm) {
+    char* t = base + (2 * n + 2 * M) * es;
+    s = fill_twiddles(c->prec, t, m1, m1, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(c->prec, t + m1 * es, m2, m2, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(c->prec, t + (m1 + m2) * es, M, nlo, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(c->prec, t + (m1 + m2 + nlo) * es, M, nhi, nlo, 0);
+    if (s != GFFT_OK) return s;
+    c->bsm = true;
+    c->gn1 = m1;
+    c->gn2 = m2;
+    c->tw1 = t;
+    c->tw2 = t + m1 * es;
+    c->bt_lo = t + (m1 + m2) * es;
+    c->bt_hi = t + (m1 + m2 + nlo) * es;
+    c->bt_shift = shift;
+  }
   const unsigned g = grid_for(std::max(n, M));
   if (c->prec == kC64) {
     k_chirp<float2><<<g, 256>>>(static_cast<float2*>(wf), n, -1);
@@ -412,7 +450,55 @@ gfft_status init_bluestein(PlanCore* c) {
   c->bs_f[0] = ff;
   c->bs_f[1] = fi;
   c->algo = Algo::Bluestein;
-  c->name = "gpu-sm100-bluestein-n" + std::to_string(n) + "-m" + std::to_string(M) + "+" + c->sub->name;
+  c->name = "gpu-sm100-bluestein-n" + std::to_string(n) + (bsm ? "-mx" : mx > 0 ? "-p2" : "") + "-m" +
+            std::to_string(M) + "+" + c->sub->name;
+  return GFFT_OK;
+}
+
+// The Bluestein chain on the compiled mixed-radix tiles (gfft_mixbs.cuh):
+// four launches per chunk of transforms, scratch and work of M elements per
+// transform each.
+static gfft_status exec_bluestein_mixed(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
+                                        int64_t idist, int64_t odist, cudaStream_t st) {
+  const size_t es = elem_bytes(c->prec);
+  const int64_t n = c->n, M = c->bm, m1 = c->gn1, m2 = c->gn2;
+  const int d = dir < 0 ? 0 : 1;
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
+  void* buf = nullptr;
+  GFFT_CUDA(ws_alloc(&buf, 2 * size_t(chunk) * size_t(M) * es, st));
+  void* scratch = buf;
+  void* work = static_cast<char*>(buf) + size_t(chunk) * size_t(M) * es;
+  const BigTwiddle bt{c->bt_lo, c->bt_hi, c->bt_shift};
+  cudaError_t e = cudaSuccess;
+  for (int64_t b0 = 0; b0 < count && e == cudaSuccess; b0 += chunk) {
+    const int64_t m = std::min(chunk, count - b0);
+    MixBsParams p{};
+    p.x = static_cast<const char*>(src) + size_t(b0) * size_t(idist) * es;
+    p.y = static_cast<char*>(dst) + size_t(b0) * size_t(odist) * es;
+    p.scratch = scratch;
+    p.work = work;
+    p.n = n;
+    p.M = M;
+    p.idist = idist;
+    p.odist = odist;
+    p.w = c->bs_w[d];
+    p.f = c->bs_f[d];
+    p.bt = bt;
+    p.scale = dir < 0 ? 1.0 : 1.0 / double(n);
+    p.inv = 0;
+    p.tw = c->tw1;
+    e = exec_mix_bs(c->prec, BSK_IN, m1, p, m, st);
+    if (e != cudaSuccess) break;
+    p.tw = c->tw2;
+    e = exec_mix_bs(c->prec, BSK_FILT, m2, p, m, st);
+    if (e != cudaSuccess) break;
+    const MixColsParams q{scratch, work, m2, m2, 0, M, M, 0, c->tw1, bt, 1.0};
+    e = exec_mix_cols(c->prec, +1, MIX_PASS1, m1, q, m, st);
+    if (e != cudaSuccess) break;
+    e = exec_mix_bs(c->prec, BSK_OUT, m2, p, m, st);
+  }
+  cudaFreeAsync(buf, st);
+  if (e != cudaSuccess) return cuda_status(e, "k_mix_bs");
   return GFFT_OK;
 }
 
@@ -421,6 +507,7 @@ static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const v
   const size_t es = elem_bytes(c->prec);
   const int64_t n = c->n, M = c->bm;
   const int d = dir < 0 ? 0 : 1;
+  if (c->bsm) return exec_bluestein_mixed(c, dir, dst, src, count, idist, odist, st);
   // one fused launch when FFT_M fits one CTA (the sub-plan is single-pass,
   // so its W_M table serves the fused stages)
   if (c->sub->algo == Algo::Pow2Smem && bluestein_fused_supported(c->prec, M)) {

@@ -14,6 +14,11 @@
 //     compiled mixed-radix column tiles: the two passes of every such
 //     transform in one launch per distinct N1 (pass 1) and one per distinct
 //     N2 (pass 2), each CTA finding its transform through an item table;
+//   - larger lengths whose Bluestein FFT can be a product M = M1 x M2 of
+//     compiled column lengths below NextPow2(2n-1): the chain of
+//     gfft_mixbs.cuh as items, four phases (chirp-load pass, filter-store
+//     pass, inverse pass 1, chirp-store pass), one launch per column length
+//     and phase, in chunks that bound the scratch;
 //   - every other larger length through Bluestein, grouped by FFT length M
 //     (NextPow2(2n-1), plan.go:865): one gather (x chirp), one batched FFT_M,
 //     one filter product, one batched inverse FFT_M, one scatter (x chirp).
@@ -27,6 +32,7 @@
 #include <new>
 #include <vector>
 #include "gfft_internal.h"
+#include "gfft_mixbs.cuh"
 #include "gfft_mixcols.cuh"
 #include "gfft_uneven.cuh"
 
@@ -115,6 +121,25 @@ struct gfft_plan_uneven {
   MixItem* d_mix_items = nullptr;
   std::vector<MixLaunch> mix_launches;  // pass-1 launches first
   int64_t mix_scratch = 0;              // elements of the intermediates
+  // Bluestein on mixed FFT lengths (item mode): per chunk of transforms,
+  // launches of the phases BSK_IN, BSK_FILT, the inverse first pass (kind
+  // kBsInv1: k_mix_cols over bsm_inv) and BSK_OUT, in that order.
+  static constexpr int kBsInv1 = 3;
+  struct BsmLaunch {
+    int kind;
+    int64_t L, tw, blocks;
+    int32_t* d_blk = nullptr;
+  };
+  struct BsmChunk {
+    int64_t elems = 0;  // M summed over the chunk's transforms
+    std::vector<BsmLaunch> launches;
+  };
+  std::vector<MixBsItem> bsm_items;
+  MixBsItem* d_bsm_items = nullptr;
+  std::vector<MixItem> bsm_inv;  // the same transforms' inverse first pass
+  MixItem* d_bsm_inv = nullptr;
+  std::vector<BsmChunk> bsm_chunks;
+  int64_t bsm_buf = 0;  // elements of the largest chunk
   // Recorded after every call's work: the next call, on whatever stream,
   // waits for it, so calls on one plan never overlap on the device (they
   // share the work buffers and queue counters above).
@@ -161,6 +186,9 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
   std::map<int64_t, int64_t> mix_n1;              // mixed-radix four-step length -> N1
   std::map<int64_t, int64_t> mix_lo, mix_hi;      // its W_n split tables
   std::map<int64_t, int> mix_shift;
+  std::map<int64_t, int64_t> bsm_M, bsm_m1;       // mixed Bluestein length n -> M, M1
+  std::map<int64_t, int64_t> bsm_lo, bsm_hi;      // W_M split tables per M
+  std::map<int64_t, int> bsm_shift;
   int64_t cursor = 0;
   auto alloc = [&](int64_t n) {
     const int64_t at = cursor;
@@ -204,6 +232,27 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     }
     int64_t M = 1;
     while (M < 2 * n - 1) M <<= 1;
+    // beyond the one-CTA kernel: a smaller FFT length of two compiled
+    // column lengths where it is at most kBsMixedRatio of M (the plans'
+    // rule; never a power of two itself)
+    int64_t bm1 = 0;
+    const int64_t mx = M > max_direct_bs ? bs_mixed_choice(n, &bm1) : 0;
+    if (mx > 0 && double(mx) <= kBsMixedRatio * double(M)) {
+      bsm_M[n] = mx;
+      bsm_m1[n] = bm1;
+      bs_by_m[mx].push_back(n);
+      chirp_off[n] = alloc(n);
+      for (int64_t L : {bm1, mx / bm1})
+        if (!tw_off.count(L)) tw_off[L] = alloc(L);
+      if (!bsm_lo.count(mx)) {
+        int shift = 0;
+        while ((int64_t(1) << (2 * shift)) < mx) ++shift;
+        bsm_shift[mx] = shift;
+        bsm_lo[mx] = alloc(int64_t(1) << shift);
+        bsm_hi[mx] = alloc((mx + (int64_t(1) << shift) - 1) >> shift);
+      }
+      continue;
+    }
     bs_by_m[M].push_back(n);
     chirp_off[n] = alloc(n);
     GenSched sm;
@@ -240,6 +289,12 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     const int64_t n = kv.first, nlo = int64_t(1) << mix_shift[n];
     gfft_status s = fill_twiddles(p->prec, tab + mix_lo[n] * es, n, nlo, 1, 0);
     if (s == GFFT_OK) s = fill_twiddles(p->prec, tab + mix_hi[n] * es, n, (n + nlo - 1) / nlo, nlo, 0);
+    if (s != GFFT_OK) return s;
+  }
+  for (auto& kv : bsm_lo) {
+    const int64_t M = kv.first, nlo = int64_t(1) << bsm_shift[M];
+    gfft_status s = fill_twiddles(p->prec, tab + bsm_lo[M] * es, M, nlo, 1, 0);
+    if (s == GFFT_OK) s = fill_twiddles(p->prec, tab + bsm_hi[M] * es, M, (M + nlo - 1) / nlo, nlo, 0);
     if (s != GFFT_OK) return s;
   }
   for (auto& kv : chirp_off) {
@@ -282,6 +337,17 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     }
     if ((n & (n - 1)) == 0) {
       p->groups[big_pow2_group[n]].items.push_back(BigItem{p->off[i], n, 0, 0});
+    } else if (bsm_M.count(n)) {
+      MixBsItem m{};
+      m.off = p->off[i];
+      m.n = n;
+      m.M = bsm_M[n];
+      m.chirp = chirp_off[n];
+      m.filt = filt_off[n];
+      m.lo = bsm_lo[m.M];
+      m.hi = bsm_hi[m.M];
+      m.shift = bsm_shift[m.M];
+      p->bsm_items.push_back(m);
     } else if (mix_n1.count(n)) {
       MixItem m{};
       m.off = p->off[i];
@@ -374,6 +440,77 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     GFFT_CUDA(cudaMemcpy(p->d_mix_items, p->mix_items.data(), p->mix_items.size() * sizeof(MixItem),
                          cudaMemcpyHostToDevice));
   }
+  // mixed Bluestein items: chunks of at most 2^27 FFT elements; per chunk one
+  // launch per column length and phase, each CTA one column tile of one item
+  if (!p->bsm_items.empty()) {
+    const int64_t kChunk = int64_t(1) << 27;
+    std::vector<std::pair<size_t, size_t>> spans;  // item ranges of the chunks
+    for (size_t i = 0; i < p->bsm_items.size();) {
+      size_t j = i;
+      int64_t sum = 0;
+      while (j < p->bsm_items.size() && (j == i || sum + p->bsm_items[j].M <= kChunk)) {
+        p->bsm_items[j].s = sum;
+        sum += p->bsm_items[j].M;
+        ++j;
+      }
+      spans.push_back({i, j});
+      gfft_plan_uneven::BsmChunk ch;
+      ch.elems = sum;
+      p->bsm_chunks.push_back(ch);
+      p->bsm_buf = std::max(p->bsm_buf, sum);
+      i = j;
+    }
+    p->bsm_inv.resize(p->bsm_items.size());
+    for (size_t i = 0; i < p->bsm_items.size(); ++i) {
+      const MixBsItem& b = p->bsm_items[i];
+      MixItem& m = p->bsm_inv[i];
+      m = MixItem{};
+      m.off = b.s;  // reads the filtered spectrum in the scratch
+      m.y = b.s;    // writes the work buffer
+      m.n = b.M;
+      m.lo = b.lo;
+      m.hi = b.hi;
+      m.shift = b.shift;
+    }
+    for (size_t ci = 0; ci < spans.size(); ++ci) {
+      for (int kind : {int(BSK_IN), int(BSK_FILT), gfft_plan_uneven::kBsInv1, int(BSK_OUT)}) {
+        const bool on_m1 = kind == BSK_IN || kind == gfft_plan_uneven::kBsInv1;
+        std::map<int64_t, std::vector<size_t>> by_len;
+        for (size_t i = spans[ci].first; i < spans[ci].second; ++i) {
+          const int64_t m1 = bsm_m1[p->bsm_items[i].n];
+          by_len[on_m1 ? m1 : p->bsm_items[i].M / m1].push_back(i);
+        }
+        for (auto& kv : by_len) {
+          const int64_t L = kv.first;
+          const int nc = kind == gfft_plan_uneven::kBsInv1 ? mix_cols_width(p->prec, MIX_PASS1, L)
+                                                          : mix_bs_width(p->prec, L);
+          if (nc <= 0) return GFFT_ERR_NOT_IMPLEMENTED;
+          std::vector<int32_t> blk;
+          for (size_t i : kv.second) {
+            const int32_t first = int32_t(blk.size());
+            if (kind == gfft_plan_uneven::kBsInv1) p->bsm_inv[i].first[0] = first;
+            else p->bsm_items[i].first[kind] = first;
+            const int64_t tiles = (p->bsm_items[i].M / L + nc - 1) / nc;
+            blk.insert(blk.end(), size_t(tiles), int32_t(i));
+          }
+          gfft_plan_uneven::BsmLaunch bl;
+          bl.kind = kind;
+          bl.L = L;
+          bl.tw = tw_off[L];
+          bl.blocks = int64_t(blk.size());
+          GFFT_CUDA(cudaMalloc(&bl.d_blk, blk.size() * sizeof(int32_t)));
+          p->bsm_chunks[ci].launches.push_back(bl);
+          GFFT_CUDA(cudaMemcpy(bl.d_blk, blk.data(), blk.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        }
+      }
+    }
+    GFFT_CUDA(cudaMalloc(&p->d_bsm_items, p->bsm_items.size() * sizeof(MixBsItem)));
+    GFFT_CUDA(cudaMemcpy(p->d_bsm_items, p->bsm_items.data(), p->bsm_items.size() * sizeof(MixBsItem),
+                         cudaMemcpyHostToDevice));
+    GFFT_CUDA(cudaMalloc(&p->d_bsm_inv, p->bsm_inv.size() * sizeof(MixItem)));
+    GFFT_CUDA(cudaMemcpy(p->d_bsm_inv, p->bsm_inv.data(), p->bsm_inv.size() * sizeof(MixItem),
+                         cudaMemcpyHostToDevice));
+  }
   GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
   GFFT_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
   GFFT_CUDA(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
@@ -407,6 +544,44 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
     }
     cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) return cuda_status(e, "k_mix_cols");
+  }
+  if (!p->bsm_items.empty()) {
+    void* buf = nullptr;
+    GFFT_CUDA(ws_alloc(&buf, 2 * size_t(p->bsm_buf) * sizeof(C), st));
+    void* scratch = buf;
+    void* work = static_cast<C*>(buf) + p->bsm_buf;
+    cudaError_t e = cudaSuccess;
+    for (const auto& ch : p->bsm_chunks) {
+      for (const auto& bl : ch.launches) {
+        const C* W = static_cast<const C*>(p->tab) + bl.tw;
+        if (bl.kind == gfft_plan_uneven::kBsInv1) {
+          MixColsParams mp{};
+          mp.src = scratch;
+          mp.dst = work;
+          mp.tw = W;
+          mp.items = p->d_bsm_inv;
+          mp.blk = bl.d_blk;
+          mp.tab = p->tab;
+          e = exec_mix_cols(p->prec, +1, MIX_PASS1, bl.L, mp, bl.blocks, st);
+        } else {
+          MixBsParams bp{};
+          bp.x = src;
+          bp.y = dst;
+          bp.scratch = scratch;
+          bp.work = work;
+          bp.tw = W;
+          bp.inv = DIR > 0;
+          bp.items = p->d_bsm_items;
+          bp.blk = bl.d_blk;
+          bp.tab = p->tab;
+          e = exec_mix_bs(p->prec, bl.kind, bl.L, bp, bl.blocks, st);
+        }
+        if (e != cudaSuccess) break;
+      }
+      if (e != cudaSuccess) break;
+    }
+    cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) return cuda_status(e, "k_mix_bs");
   }
   for (Group& g : p->groups) {
     const int64_t rows = int64_t(g.items.size());
@@ -533,6 +708,11 @@ void gfft_plan_uneven_close(gfft_plan_uneven* p) {
   for (auto& ml : p->mix_launches)
     if (ml.d_blk) cudaFree(ml.d_blk);
   if (p->d_mix_items) cudaFree(p->d_mix_items);
+  for (auto& ch : p->bsm_chunks)
+    for (auto& bl : ch.launches)
+      if (bl.d_blk) cudaFree(bl.d_blk);
+  if (p->d_bsm_items) cudaFree(p->d_bsm_items);
+  if (p->d_bsm_inv) cudaFree(p->d_bsm_inv);
   if (p->d_descs) cudaFree(p->d_descs);
   if (p->tab) cudaFree(p->tab);
   if (p->counters) cudaFree(p->counters);

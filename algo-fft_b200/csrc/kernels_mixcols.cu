@@ -1,6 +1,7 @@
 // The compiled mixed-radix column tiles (gfft_mixcols.cuh) of every 7-smooth
-// column length 48..1024: the table the generated kernels_mixcols_t*.cu files
-// fill, and the launcher the four-step and column-batch plans call.
+// column length 48..1024 and the Bluestein chain's passes on them
+// (gfft_mixbs.cuh): the tables the generated kernels_mixcols_t*.cu and
+// kernels_mixbs_t*.cu files fill, and the launchers the plans call.
 #include <algorithm>
 #include "kernels_mixcols.cuh"
 
@@ -14,6 +15,9 @@ void mix_part_4(std::vector<MixEntry>& v);
 void mix_part_5(std::vector<MixEntry>& v);
 void mix_part_6(std::vector<MixEntry>& v);
 void mix_part_7(std::vector<MixEntry>& v);
+void mix_bs_part_0(std::vector<MixBsEntry>& v);
+void mix_bs_part_1(std::vector<MixBsEntry>& v);
+void mix_bs_part_2(std::vector<MixBsEntry>& v);
 
 namespace {
 
@@ -35,9 +39,59 @@ const MixEntry* find(int64_t L) {
   return it != t.end() && it->L == L ? &*it : nullptr;
 }
 
+const std::vector<MixBsEntry>& bs_table() {
+  static const std::vector<MixBsEntry> t = [] {
+    std::vector<MixBsEntry> v;
+    for (auto part : {&mix_bs_part_0, &mix_bs_part_1, &mix_bs_part_2}) part(v);
+    std::sort(v.begin(), v.end(), [](const MixBsEntry& a, const MixBsEntry& b) { return a.L < b.L; });
+    return v;
+  }();
+  return t;
+}
+
+const MixBsEntry* bs_find(int64_t L) {
+  for (const MixBsEntry& e : bs_table())
+    if (e.L == L) return &e;
+  return nullptr;
+}
+
 }  // namespace
 
 bool mix_cols_supported(int64_t L) { return find(L) != nullptr; }
+
+int64_t bs_mixed_length(int64_t n, int64_t* m1) {
+  int64_t best = 0, a_best = 0;
+  const std::vector<MixBsEntry>& t = bs_table();
+  for (size_t i = 0; i < t.size(); ++i)
+    for (size_t j = i; j < t.size(); ++j) {
+      const int64_t a = t[i].L, b = t[j].L, m = a * b;
+      if (m < 2 * n - 1) continue;
+      // the smallest M; among equal ones the most balanced split
+      if (best == 0 || m < best || (m == best && a > a_best)) {
+        best = m;
+        a_best = a;
+      }
+    }
+  if (m1) *m1 = a_best;
+  return best;
+}
+
+int mix_bs_width(int prec, int64_t L) {
+  const MixBsEntry* e = bs_find(L);
+  return e && (prec == kC64 || prec == kC128) ? e->nc[prec] : 0;
+}
+
+cudaError_t exec_mix_bs(int prec, int kind, int64_t L, MixBsParams p, int64_t count, cudaStream_t st) {
+  const MixBsEntry* e = bs_find(L);
+  if (!e || kind < BSK_IN || kind > BSK_OUT || (prec != kC64 && prec != kC128)) return cudaErrorNotSupported;
+  int64_t blocks = count;  // item mode: CTAs
+  if (!p.items) {
+    const int nc = e->nc[prec];
+    p.tiles = (p.M / L + nc - 1) / nc;
+    blocks = p.tiles * count;
+  }
+  return e->fn[prec][kind](p, blocks, st);
+}
 
 std::vector<int64_t> mix_cols_lengths() {
   std::vector<int64_t> v;

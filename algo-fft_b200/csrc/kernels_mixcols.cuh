@@ -1,9 +1,11 @@
 // Launchers and table entries of the compiled mixed-radix column tiles
-// (gfft_mixcols.cuh).  The generated kernels_mixcols_t*.cu files each
-// instantiate a share of the table (gen_mixcols.py picks the schedules);
+// (gfft_mixcols.cuh) and of the Bluestein chain on them (gfft_mixbs.cuh).
+// The generated kernels_mixcols_t*.cu / kernels_mixbs_t*.cu files each
+// instantiate a share of the tables (gen_mixcols.py picks the schedules);
 // kernels_mixcols.cu gathers them.
 #pragma once
 #include "gfft_internal.h"
+#include "gfft_mixbs.cuh"
 #include "gfft_mixcols.cuh"
 
 namespace gfft {
@@ -62,6 +64,49 @@ MixEntry mix_entry() {
   e.fn[kC128][0][1] = &launch_mix<double2, D2, -1, MIX_PASS2>;
   e.fn[kC128][1][0] = &launch_mix<double2, D1, +1, MIX_PASS1>;
   e.fn[kC128][1][1] = &launch_mix<double2, D2, +1, MIX_PASS2>;
+  return e;
+}
+
+
+using MixBsFn = cudaError_t (*)(const MixBsParams&, int64_t, cudaStream_t);
+
+struct MixBsEntry {
+  int L;
+  int nc[2];           // tile width per precision
+  MixBsFn fn[2][3];    // [prec][BSK_IN / BSK_FILT / BSK_OUT]
+};
+
+template <typename C, typename CFG, int KIND>
+cudaError_t launch_mix_bs(const MixBsParams& p, int64_t blocks, cudaStream_t st) {
+  using SC = typename CFG::Sched;
+  constexpr int NC = CFG::nc;
+  using TL = MixTile<SC, NC, CFG::tt>;
+  constexpr int smem = (KIND == BSK_IN ? TL::ELEMS1 : TL::ELEMS2) * int(sizeof(C));
+  auto kern = &k_mix_bs<C, SC, NC, KIND, CFG::minb, CFG::tt>;
+  static const cudaError_t attr =
+      smem > 48 * 1024 ? cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) : cudaSuccess;
+  if (attr != cudaSuccess) return attr;
+  if (blocks <= 0) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  kern<<<unsigned(blocks), TL::TPB, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+// Bluestein-chain entry of length L from its complex64 and complex128
+// configurations (the column tiles' own).
+template <typename F, typename D>
+MixBsEntry mix_bs_entry() {
+  static_assert(F::Sched::L == D::Sched::L, "one length per entry");
+  MixBsEntry e{};
+  e.L = F::Sched::L;
+  e.nc[kC64] = F::nc;
+  e.nc[kC128] = D::nc;
+  e.fn[kC64][BSK_IN] = &launch_mix_bs<float2, F, BSK_IN>;
+  e.fn[kC64][BSK_FILT] = &launch_mix_bs<float2, F, BSK_FILT>;
+  e.fn[kC64][BSK_OUT] = &launch_mix_bs<float2, F, BSK_OUT>;
+  e.fn[kC128][BSK_IN] = &launch_mix_bs<double2, D, BSK_IN>;
+  e.fn[kC128][BSK_FILT] = &launch_mix_bs<double2, D, BSK_FILT>;
+  e.fn[kC128][BSK_OUT] = &launch_mix_bs<double2, D, BSK_OUT>;
   return e;
 }
 

@@ -657,7 +657,7 @@ def _convolve(dev, stream, iters, gen):
     return out
 
 
-CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
+CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "bs_mixed", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
          "gen_cols", "mix_cols", "tp3t", "tp2", "p16384")
 
 
@@ -692,12 +692,14 @@ def run_case(name: str, reps: int) -> int:
         x = cplx(p.Total())
         y = torch.empty_like(x)
         fn = lambda: p.Forward(y, x)  # noqa: E731
-    elif name in ("bs_fused", "bs_tp"):  # Bluestein: n = 8191 (M = 16384, one CTA) / 16411 (M = 65536)
+    elif name in ("bs_fused", "bs_tp", "bs_mixed"):
+        # Bluestein: n = 8191 (M = 16384, one CTA) / 16411 on M = 65536 (the two-pass power-of-two
+        # chain) / 16411 on M = 34560 = 144 x 240 (the mixed-radix chain)
         n = 8191 if name == "bs_fused" else 16411
         count = (1 << 27) // (8 * n)
         x = cplx(n * count)
         y = torch.empty_like(x)
-        p = algofft.NewPlan(n)
+        p = algofft.Plan(n, variant=f"gpu-sm100-bluestein-n{n}-p2") if name == "bs_tp" else algofft.NewPlan(n)
         close.append(p)
         fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
     elif name == "conv_os":  # ConvolveReal, 8 signals of 2^20 reals with a 4097-tap kernel

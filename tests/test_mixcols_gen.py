@@ -23,10 +23,17 @@ def _gen():
 def test_generated_files_are_current(tmp_path):
     g = _gen()
     g.main(str(tmp_path))
-    for k in range(g.PARTS):
-        name = f"kernels_mixcols_t{k}.cu"
+    names = [f"kernels_mixcols_t{k}.cu" for k in range(g.PARTS)] + [f"kernels_mixbs_t{k}.cu" for k in range(g.BS_PARTS)]
+    for name in names:
         with open(os.path.join(CSRC, name)) as a, open(tmp_path / name) as b:
             assert a.read() == b.read(), f"{name} is stale: run gen_mixcols.py"
+
+
+def test_bluestein_lengths_are_table_lengths():
+    g = _gen()
+    bs = g.bs_lengths()
+    assert bs == [L for L in range(48, 513) if g.smooth7(L) and L % 16 == 0] and len(bs) == 21
+    assert max(bs) ** 2 == 1 << 18  # FFT lengths up to 2^18: n up to 131072
 
 
 def test_every_length_has_a_launchable_plan():
