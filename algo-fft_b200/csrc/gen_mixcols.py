@@ -75,11 +75,11 @@ def vmax(L, sched, T):
     return max(-(-(L // r) // T) * r for r in sched)
 
 
-def minb(L, sched, nc, es, T):
+def minb(L, sched, nc, es, T, extra=0):
     tpb = T * nc
     tpbw = -(-tpb // 32) * 32
     per = 2 * (es // 8)  # registers per complex value
-    regs = int(per * vmax(L, sched, T) * (1.0 if es == 8 else 1.3)) + 40
+    regs = int(per * vmax(L, sched, T) * (1.0 if es == 8 else 1.3)) + 40 + extra
     pitch = nc + 1 if nc >= 16 else nc
     smem = max(L * pitch, nc * (L | 1)) * es
     k = 1
@@ -89,17 +89,18 @@ def minb(L, sched, nc, es, T):
     return k
 
 
-def plan(L, es):
-    """(radices, tile width, MINB, threads per column or 0) of one pass."""
+def plan(L, es, extra=0):
+    """(radices, tile width, MINB, threads per column or 0) of one pass;
+    `extra` registers per thread added to the occupancy estimate."""
     sched = schedule(L)
     nc = (16 if L < 500 else 8) if es == 8 else (8 if L < 500 else 4)
     wide = sched[0] % sched[1] != 0 and L in WIDE[es]
     T = threads(L, sched, wide)
-    return sched, nc, minb(L, sched, nc, es, T), T if wide else 0
+    return sched, nc, minb(L, sched, nc, es, T, extra), T if wide else 0
 
 
-def cfg(L, es):
-    sched, nc, mb, tt = plan(L, es)
+def cfg(L, es, extra=0):
+    sched, nc, mb, tt = plan(L, es, extra)
     s = ", ".join(str(r) for r in sched)
     return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
 

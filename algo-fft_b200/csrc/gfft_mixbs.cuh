@@ -85,7 +85,9 @@ struct MixBsFilt {
   int inv;
   __device__ __forceinline__ void store(int row, int c, C v) const {
     const int64_t k = col0 + c + m1 * int64_t(row);
-    const C fk = inv ? cconj(__ldg(f + (k == 0 ? 0 : M - k))) : __ldg(f + k);
+    // one load per element: the index first, then the conjugate
+    C fk = __ldg(f + (inv ? (k == 0 ? 0 : M - k) : k));
+    if (inv) fk.y = -fk.y;
     __stcg(z + k, cmul(v, fk));
   }
 };

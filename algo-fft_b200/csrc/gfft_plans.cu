@@ -463,7 +463,10 @@ static gfft_status exec_bluestein_mixed(const PlanCore* c, int dir, void* dst, c
   const size_t es = elem_bytes(c->prec);
   const int64_t n = c->n, M = c->bm, m1 = c->gn1, m2 = c->gn2;
   const int d = dir < 0 ? 0 : 1;
-  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
+  // chunks of at most 512 MB per buffer, of equal size (no short tail chunk)
+  const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(512) << 20) / (M * int64_t(es))));
+  const int64_t nchunks = (count + cap - 1) / cap;
+  const int64_t chunk = (count + nchunks - 1) / nchunks;
   void* buf = nullptr;
   GFFT_CUDA(ws_alloc(&buf, 2 * size_t(chunk) * size_t(M) * es, st));
   void* scratch = buf;
