@@ -392,13 +392,33 @@ bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* toke
   std::lock_guard<std::mutex> g(M.mu);
   model_try_default();
   if (!M.loaded) return false;
-  // candidates of a kind the model has no features for (variant families
-  // added after it was trained) are left out
+  // Variant families added after the model was trained are scored as the
+  // family they refine: the compiled mixed-radix four-step ("-mixc-AxB") with
+  // the features of the runtime-radix split AxB, replacing the runtime
+  // four-step it outruns (2-3x at every length measured); Bluestein's two FFT
+  // lengths ("-mx" / "-p2") as one Bluestein candidate whose length the
+  // plan's own rule picks.  Candidates of any other unknown kind are left out.
+  const std::vector<std::string> cands = variant_tokens(prec, n);
+  bool has_mixc = false;
+  for (const std::string& t : cands) has_mixc |= t.find("-mixc-") != std::string::npos;
+  const std::string bs_plain = "gpu-sm100-bluestein-n" + std::to_string(n);
+  bool bs_added = false;
   std::vector<std::string> toks;
   std::vector<float> xs;
-  for (const std::string& t : variant_tokens(prec, n)) {
+  for (const std::string& t0 : cands) {
+    std::string t = t0, ft = t0;
+    const size_t mc = t0.find("-mixc-");
+    if (mc != std::string::npos) {
+      ft = "gpu-sm100-mixed2-" + t0.substr(mc + 6);
+    } else if (has_mixc && t0.rfind("gpu-sm100-mixed2-", 0) == 0) {
+      continue;
+    } else if (t0 == bs_plain + "-mx" || t0 == bs_plain + "-p2") {
+      if (bs_added) continue;
+      bs_added = true;
+      t = ft = bs_plain;
+    }
     float f[D];
-    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, t, f)) continue;
+    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, ft, f)) continue;
     for (int d = 0; d < D; ++d) xs.push_back((f[d] - M.norm[d]) / M.norm[D + d]);
     toks.push_back(t);
   }

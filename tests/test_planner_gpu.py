@@ -114,3 +114,26 @@ def test_learned_plan_creation_picks_a_variant_and_transforms():
         algofft.check(algofft.lib().gfft_planner_set_model(None, None))
         algofft.ClearWisdom()
         algofft.ImportWisdomFromString(saved)
+
+
+def test_learned_pick_scores_new_families_as_the_ones_they_refine():
+    """With the shipped model: a 7-smooth two-pass length never gets the
+    runtime-radix split when the compiled mixed-radix one exists (scored with
+    its features, it replaces it), and a prime with the two Bluestein lengths
+    is one candidate, so the model defers to the size-class rules."""
+    saved = algofft.ExportWisdomToString()
+    algofft.ClearWisdom()
+    P.Model.load(P.DEFAULT_MODEL).install()
+    try:
+        for n in (50421, 100000):
+            buf = ctypes.create_string_buffer(128)
+            algofft.check(algofft.lib().gfft_planner_choose(0, n, 16, 1, 0, buf, 128))
+            tok = buf.value.decode()
+            assert "-mixed2-" not in tok and tok in algofft.Variants(n), tok
+        buf = ctypes.create_string_buffer(128)
+        assert algofft.lib().gfft_planner_choose(0, 16411, 16, 1, 0, buf, 128) != 0
+        with algofft.NewPlanWithOptions(16411, algofft.PlanOptions(Planner=algofft.PlannerLearned)) as pl:
+            assert pl.Algorithm().startswith("gpu-sm100-bluestein-n16411-mx-")
+    finally:
+        algofft.ClearWisdom()
+        algofft.ImportWisdomFromString(saved)
