@@ -1,6 +1,9 @@
 """Writes kernels_mixcols_t0.cu .. kernels_mixcols_t7.cu: the compiled
 mixed-radix column tiles (gfft_mixcols.cuh) of every 7-smooth column length
 48 <= L <= 1024, spread over eight files so nvcc builds them in parallel; and
+kernels_mixrows_t0.cu .. kernels_mixrows_t3.cu: the same schedules in rows
+mode (k_mix_rows: whole contiguous transforms of every table length, several
+per CTA, the single-pass plans of those lengths); and
 kernels_mixbs_t0.cu .. kernels_mixbs_t2.cu: the Bluestein chain's passes
 (gfft_mixbs.cuh) for the column lengths its FFT lengths M = M1 x M2 are built
 from (BS_LENGTHS: the multiples of 16 up to 512, whose products come within
@@ -30,6 +33,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 PARTS = 8
 BS_PARTS = 3
+ROW_PARTS = 4
 
 
 def smooth7(n):
@@ -99,6 +103,33 @@ def plan(L, es, extra=0):
     return sched, nc, minb(L, sched, nc, es, T, extra), T if wide else 0
 
 
+def rows_plan(L, es):
+    """Rows mode: the column schedule and thread layout; transforms per CTA
+    (a power of two) as many as keep the CTA within 512 threads and 64 KB of
+    shared memory; resident CTAs per SM by the same register estimate, up to
+    2048 threads and 200 KB per SM."""
+    sched, _, _, tt = plan(L, es)
+    T = tt if tt else L // max(sched)
+    nc = 1
+    while nc < 64 and T * nc * 2 <= 512 and 2 * nc * (L | 1) * es <= 64 * 1024:
+        nc *= 2
+    tpb = T * nc
+    tpbw = -(-tpb // 32) * 32
+    regs = int(2 * (es // 8) * vmax(L, sched, T) * (1.0 if es == 8 else 1.3)) + 40
+    smem = nc * (L | 1) * es
+    k = 1
+    while (k < 8 and 65536 // ((k + 1) * tpbw) >= regs and (k + 1) * tpb <= 2048
+           and (k + 1) * smem <= 200 * 1024):
+        k += 1
+    return sched, nc, k, tt
+
+
+def rows_cfg(L, es):
+    sched, nc, mb, tt = rows_plan(L, es)
+    s = ", ".join(str(r) for r in sched)
+    return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
+
+
 def cfg(L, es, extra=0):
     sched, nc, mb, tt = plan(L, es, extra)
     s = ", ".join(str(r) for r in sched)
@@ -122,6 +153,14 @@ def main(out=HERE):
             fh.write("// Generated by gen_mixcols.py; do not edit.\n"
                      "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
                      f"void mix_part_{k}(std::vector<MixEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
+    rparts = [[] for _ in range(ROW_PARTS)]
+    for i, L in enumerate(lengths):
+        rparts[i % ROW_PARTS].append(f"  v.push_back(mix_rows_entry<{rows_cfg(L, 8)},\n                              {rows_cfg(L, 16)}>());  // {L}\n")
+    for k, body in enumerate(rparts):
+        with open(os.path.join(out, f"kernels_mixrows_t{k}.cu"), "w") as fh:
+            fh.write("// Generated by gen_mixcols.py; do not edit.\n"
+                     "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
+                     f"void mix_rows_part_{k}(std::vector<MixRowsEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
     bparts = [[] for _ in range(BS_PARTS)]
     for i, L in enumerate(bs_lengths()):
         bparts[i % BS_PARTS].append(f"  v.push_back(mix_bs_entry<{cfg(L, 8)},\n                            {cfg(L, 16)}>());  // {L}\n")

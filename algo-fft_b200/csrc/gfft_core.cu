@@ -445,6 +445,7 @@ gfft_status core_init_variant(PlanCore* c, int prec, int64_t n, int device, cons
   }
   long long ln = 0, l1 = 0, l2 = 0;
   if (std::sscanf(tok.c_str(), "gpu-sm100-mixed-n%lld", &ln) == 1 && ln == n && is_smooth7(n)) return init_generic(c);
+  if (std::sscanf(tok.c_str(), "gpu-sm100-mixr-n%lld", &ln) == 1 && ln == n && is_smooth7(n)) return init_generic(c, true);
   if (std::sscanf(tok.c_str(), "gpu-sm100-mixed2-%lldx%lld", &l1, &l2) == 2 && l1 * l2 == n && is_smooth7(n)) {
     gfft_status s = init_gen_twopass(c);
     if (s == GFFT_OK && c->gn1 == l1) return s;
@@ -554,7 +555,10 @@ gfft_status core_init(PlanCore* c, int prec, int64_t n, int device, int strategy
   // when it fits, else two passes); everything else, or a forced
   // KernelBluestein, goes through Bluestein (planner.go:50-55).
   if (strategy != GFFT_KERNEL_BLUESTEIN && is_smooth7(n)) {
-    gfft_status s = init_generic(c);
+    gfft_status s = init_generic(c, true);
+    if (s == GFFT_OK) return s;
+    core_free(c);
+    s = init_generic(c);
     if (s == GFFT_OK) return s;
     core_free(c);
     s = init_gen_twopass(c, true);
@@ -587,6 +591,7 @@ void core_free(PlanCore* c) {
     c->sub = nullptr;
   }
   c->mixc = false;
+  c->mixr = false;
   c->bsm = false;
   c->algo = Algo::Trivial;
 }

@@ -85,6 +85,7 @@ struct PlanCore {
   GenSched gs{}, gs1{}, gs2{};
   int64_t gn1 = 0, gn2 = 0;
   bool mixc = false;  // two passes on the compiled mixed-radix column tiles
+  bool mixr = false;  // one pass on the compiled tiles in rows mode (Algo::Generic)
   // Bluestein: chirps and filters per direction, sub-plan of length bm;
   // bsm: bm = gn1 x gn2 on the compiled mixed-radix tiles (tw1 = W_gn1,
   // tw2 = W_gn2, bt_* = W_bm split)
@@ -99,7 +100,7 @@ bool is_smooth7(int64_t n);
 // Runtime Stockham schedule of a 7-smooth n (false when n is not 7-smooth or
 // needs more than 1024 threads).
 bool make_gen_sched(int64_t n, GenSched* s);
-gfft_status init_generic(PlanCore* c);
+gfft_status init_generic(PlanCore* c, bool mixr = false);
 // Variant tokens of the runtime-radix schedules that can serve n.
 std::vector<std::string> mixed_tokens(int prec, int64_t n);
 // mixc: split n into two lengths with compiled mixed-radix column tiles
@@ -122,6 +123,10 @@ cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams 
 // 0 when none), and one of its passes (BSK_IN / BSK_FILT / BSK_OUT) over
 // `count` transforms, or `count` CTAs in item mode.
 struct MixBsParams;
+// Whole contiguous transforms of a compiled column length (rows mode).
+struct MixRowsParams;
+bool mix_rows_supported(int64_t L);
+cudaError_t exec_mix_rows(int prec, int dir, int64_t L, const MixRowsParams& p, cudaStream_t st);
 int64_t bs_mixed_length(int64_t n, int64_t* m1);
 int mix_bs_width(int prec, int64_t L);
 cudaError_t exec_mix_bs(int prec, int kind, int64_t L, MixBsParams p, int64_t count, cudaStream_t st);

@@ -304,3 +304,64 @@ __global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_cols(Mix
 }
 
 }  // namespace gfft
+
+namespace gfft {
+
+// Rows mode: NC whole contiguous transforms of length L per CTA, thread t of
+// transform c at tid = c * T + t (consecutive threads walk one transform, so
+// every load and store is coalesced); transform c's elements at c * LP + row
+// in shared memory (LP odd: a warp's consecutive rows fall in distinct banks).
+template <typename SC, int NC, int TT = 0>
+struct MixTileRows {
+  static constexpr int L = SC::L;
+  static constexpr int T = TT > 0 ? TT : L / SC::rmax();
+  static constexpr int TPB = T * NC;
+  static_assert(TPB <= 1024, "tile needs more than 1024 threads");
+  static constexpr int LP = L | 1;
+  static constexpr int ELEMS = NC * LP;
+  __host__ __device__ static constexpr int q_at(int s) { return (L / SC::radix(s) + T - 1) / T; }
+  __host__ __device__ static constexpr int vmax() {
+    int m = 1;
+    for (int s = 0; s < SC::NS; ++s) m = q_at(s) * SC::radix(s) > m ? q_at(s) * SC::radix(s) : m;
+    return m;
+  }
+  __device__ static __forceinline__ int phys(int row, int c) { return c * LP + row; }
+};
+
+struct MixRowsParams {
+  const void* src;
+  void* dst;
+  int64_t count, idist, odist;
+  const void* tw;  // W_L^m, m < L
+  double scale;    // 1/L for the inverse
+};
+
+template <typename C>
+struct MixRowsIO {
+  static constexpr bool kLoad = true, kStore = true;
+  const C* x;
+  C* y;
+  int64_t idist, odist;
+  __device__ __forceinline__ C load(int row, int c) const { return ld_stream(x + c * idist + row); }
+  __device__ __forceinline__ void store(int row, int c, C v) const { st_stream(y + c * odist + row, v); }
+};
+
+// One CTA per NC consecutive transforms (the last CTA masks the missing ones).
+template <typename C, typename SC, int NC, int DIR, int MINB = 1, int TT = 0>
+__global__ void __launch_bounds__(MixTileRows<SC, NC, TT>::TPB, MINB) k_mix_rows(MixRowsParams p) {
+  using TL = MixTileRows<SC, NC, TT>;
+  using Re = typename RealOf<C>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sh = reinterpret_cast<C*>(smem_raw);
+  const int64_t b0 = int64_t(blockIdx.x) * NC;
+  const int c = threadIdx.x / TL::T, t = threadIdx.x % TL::T;
+  const bool active = b0 + c < p.count;
+  const MixRowsIO<C> io{static_cast<const C*>(p.src) + b0 * p.idist, static_cast<C*>(p.dst) + b0 * p.odist, p.idist,
+                        p.odist};
+  C v[TL::vmax()];
+  mix_stage<C, SC, TL, DIR, 0, MIX_PASS2, MixRowsIO<C>>(v, nullptr, nullptr, sh, t, c, active,
+                                                        static_cast<const C*>(p.tw), Re(p.scale), BigTwiddle{}, 0,
+                                                        0, 0, io);
+}
+
+}  // namespace gfft

@@ -395,12 +395,16 @@ bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* toke
   // Variant families added after the model was trained are scored as the
   // family they refine: the compiled mixed-radix four-step ("-mixc-AxB") with
   // the features of the runtime-radix split AxB, replacing the runtime
-  // four-step it outruns (2-3x at every length measured); Bluestein's two FFT
+  // four-step it outruns (2-3x at every length measured), the compiled
+  // single pass ("-mixr-nN") likewise for the runtime one; Bluestein's two FFT
   // lengths ("-mx" / "-p2") as one Bluestein candidate whose length the
   // plan's own rule picks.  Candidates of any other unknown kind are left out.
   const std::vector<std::string> cands = variant_tokens(prec, n);
-  bool has_mixc = false;
-  for (const std::string& t : cands) has_mixc |= t.find("-mixc-") != std::string::npos;
+  bool has_mixc = false, has_mixr = false;
+  for (const std::string& t : cands) {
+    has_mixc |= t.find("-mixc-") != std::string::npos;
+    has_mixr |= t.find("-mixr-") != std::string::npos;
+  }
   const std::string bs_plain = "gpu-sm100-bluestein-n" + std::to_string(n);
   bool bs_added = false;
   std::vector<std::string> toks;
@@ -408,9 +412,13 @@ bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* toke
   for (const std::string& t0 : cands) {
     std::string t = t0, ft = t0;
     const size_t mc = t0.find("-mixc-");
+    const size_t mr = t0.find("-mixr-");
     if (mc != std::string::npos) {
       ft = "gpu-sm100-mixed2-" + t0.substr(mc + 6);
-    } else if (has_mixc && t0.rfind("gpu-sm100-mixed2-", 0) == 0) {
+    } else if (mr != std::string::npos) {
+      ft = "gpu-sm100-mixed-" + t0.substr(mr + 6);
+    } else if ((has_mixc && t0.rfind("gpu-sm100-mixed2-", 0) == 0) ||
+               (has_mixr && t0.rfind("gpu-sm100-mixed-n", 0) == 0)) {
       continue;
     } else if (t0 == bs_plain + "-mx" || t0 == bs_plain + "-p2") {
       if (bs_added) continue;

@@ -182,10 +182,22 @@ static cudaError_t prepare_generic_kernels() {
 // -------------------------------------------------------- 7-smooth plans
 
 // Single-CTA schedule when one transform (T <= 1024 threads, shared memory
-// within budget) fits; B transforms per CTA up to 256 threads.
-gfft_status init_generic(PlanCore* c) {
+// within budget) fits; B transforms per CTA up to 256 threads.  mixr: the
+// compiled mixed-radix schedule of the length in rows mode instead (7-smooth
+// lengths 48..1024).
+gfft_status init_generic(PlanCore* c, bool mixr) {
   GenSched s;
   const size_t es = elem_bytes(c->prec);
+  if (mixr) {
+    if (!mix_rows_supported(c->n)) return GFFT_ERR_NOT_IMPLEMENTED;
+    gfft_status st = make_twiddles(c->prec, c->n, &c->tw, 0);
+    if (st != GFFT_OK) return st;
+    GFFT_CUDA(cudaStreamSynchronize(0));
+    c->mixr = true;
+    c->algo = Algo::Generic;
+    c->name = "gpu-sm100-mixr-n" + std::to_string(c->n);
+    return GFFT_OK;
+  }
   if (!make_sched(c->n, &s) || size_t(s.stride) * es > size_t(kSmemBudget)) return GFFT_ERR_NOT_IMPLEMENTED;
   s.B = std::max(1, std::min(256 / s.T, int(kSmemBudget / (size_t(s.stride) * es))));
   GFFT_CUDA(prepare_generic_kernels());
@@ -229,6 +241,7 @@ std::vector<std::string> mixed_tokens(int prec, int64_t n) {
   const size_t es = elem_bytes(prec);
   GenSched s, s1, s2;
   if (make_sched(n, &s) && size_t(s.stride) * es <= size_t(kSmemBudget)) v.push_back("gpu-sm100-mixed-n" + std::to_string(n));
+  if (mix_rows_supported(n)) v.push_back("gpu-sm100-mixr-n" + std::to_string(n));
   const int64_t n1 = gen_split(n), n2 = n / n1;
   const int want = prec == kC64 ? 16 : 8;
   if (n1 >= 2 && make_col_sched(n1, es, want, &s1) && make_col_sched(n2, es, want, &s2))
@@ -582,6 +595,12 @@ gfft_status exec_runtime_plan(const PlanCore* c, int dir, void* dst, const void*
                               int64_t odist, cudaStream_t st) {
   switch (c->algo) {
     case Algo::Generic:
+      if (c->mixr) {
+        MixRowsParams p{src, dst, count, idist, odist, c->tw, dir < 0 ? 1.0 : 1.0 / double(c->n)};
+        const cudaError_t e = exec_mix_rows(c->prec, dir, c->n, p, st);
+        if (e != cudaSuccess) return cuda_status(e, "k_mix_rows");
+        return GFFT_OK;
+      }
       GFFT_CUDA(c->prec == kC64 ? launch_generic<float2>(c, dir, src, dst, count, idist, odist, st)
                                 : launch_generic<double2>(c, dir, src, dst, count, idist, odist, st));
       return GFFT_OK;

@@ -15,6 +15,10 @@ void mix_part_4(std::vector<MixEntry>& v);
 void mix_part_5(std::vector<MixEntry>& v);
 void mix_part_6(std::vector<MixEntry>& v);
 void mix_part_7(std::vector<MixEntry>& v);
+void mix_rows_part_0(std::vector<MixRowsEntry>& v);
+void mix_rows_part_1(std::vector<MixRowsEntry>& v);
+void mix_rows_part_2(std::vector<MixRowsEntry>& v);
+void mix_rows_part_3(std::vector<MixRowsEntry>& v);
 void mix_bs_part_0(std::vector<MixBsEntry>& v);
 void mix_bs_part_1(std::vector<MixBsEntry>& v);
 void mix_bs_part_2(std::vector<MixBsEntry>& v);
@@ -37,6 +41,22 @@ const MixEntry* find(int64_t L) {
   const std::vector<MixEntry>& t = table();
   auto it = std::lower_bound(t.begin(), t.end(), L, [](const MixEntry& e, int64_t l) { return e.L < l; });
   return it != t.end() && it->L == L ? &*it : nullptr;
+}
+
+const std::vector<MixRowsEntry>& rows_table() {
+  static const std::vector<MixRowsEntry> t = [] {
+    std::vector<MixRowsEntry> v;
+    for (auto part : {&mix_rows_part_0, &mix_rows_part_1, &mix_rows_part_2, &mix_rows_part_3}) part(v);
+    std::sort(v.begin(), v.end(), [](const MixRowsEntry& a, const MixRowsEntry& b) { return a.L < b.L; });
+    return v;
+  }();
+  return t;
+}
+
+const MixRowsEntry* rows_find(int64_t L) {
+  for (const MixRowsEntry& e : rows_table())
+    if (e.L == L) return &e;
+  return nullptr;
 }
 
 const std::vector<MixBsEntry>& bs_table() {
@@ -74,6 +94,14 @@ int64_t bs_mixed_length(int64_t n, int64_t* m1) {
     }
   if (m1) *m1 = a_best;
   return best;
+}
+
+bool mix_rows_supported(int64_t L) { return rows_find(L) != nullptr; }
+
+cudaError_t exec_mix_rows(int prec, int dir, int64_t L, const MixRowsParams& p, cudaStream_t st) {
+  const MixRowsEntry* e = rows_find(L);
+  if (!e || (prec != kC64 && prec != kC128)) return cudaErrorNotSupported;
+  return e->fn[prec][dir < 0 ? 0 : 1](p, st);
 }
 
 int mix_bs_width(int prec, int64_t L) {

@@ -110,4 +110,43 @@ MixBsEntry mix_bs_entry() {
   return e;
 }
 
+using MixRowsFn = cudaError_t (*)(const MixRowsParams&, cudaStream_t);
+
+struct MixRowsEntry {
+  int L;
+  int nc[2];           // transforms per CTA per precision
+  MixRowsFn fn[2][2];  // [prec][dir < 0 ? 0 : 1]
+};
+
+template <typename C, typename CFG, int DIR>
+cudaError_t launch_mix_rows(const MixRowsParams& p, cudaStream_t st) {
+  using SC = typename CFG::Sched;
+  constexpr int NC = CFG::nc;
+  using TL = MixTileRows<SC, NC, CFG::tt>;
+  constexpr int smem = TL::ELEMS * int(sizeof(C));
+  auto kern = &k_mix_rows<C, SC, NC, DIR, CFG::minb, CFG::tt>;
+  static const cudaError_t attr =
+      smem > 48 * 1024 ? cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) : cudaSuccess;
+  if (attr != cudaSuccess) return attr;
+  const int64_t blocks = (p.count + NC - 1) / NC;
+  if (blocks <= 0) return cudaSuccess;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  kern<<<unsigned(blocks), TL::TPB, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename F, typename D>
+MixRowsEntry mix_rows_entry() {
+  static_assert(F::Sched::L == D::Sched::L, "one length per entry");
+  MixRowsEntry e{};
+  e.L = F::Sched::L;
+  e.nc[kC64] = F::nc;
+  e.nc[kC128] = D::nc;
+  e.fn[kC64][0] = &launch_mix_rows<float2, F, -1>;
+  e.fn[kC64][1] = &launch_mix_rows<float2, F, +1>;
+  e.fn[kC128][0] = &launch_mix_rows<double2, D, -1>;
+  e.fn[kC128][1] = &launch_mix_rows<double2, D, +1>;
+  return e;
+}
+
 }  // namespace gfft

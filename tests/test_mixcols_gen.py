@@ -23,7 +23,8 @@ def _gen():
 def test_generated_files_are_current(tmp_path):
     g = _gen()
     g.main(str(tmp_path))
-    names = [f"kernels_mixcols_t{k}.cu" for k in range(g.PARTS)] + [f"kernels_mixbs_t{k}.cu" for k in range(g.BS_PARTS)]
+    names = ([f"kernels_mixcols_t{k}.cu" for k in range(g.PARTS)] + [f"kernels_mixbs_t{k}.cu" for k in range(g.BS_PARTS)]
+             + [f"kernels_mixrows_t{k}.cu" for k in range(g.ROW_PARTS)])
     for name in names:
         with open(os.path.join(CSRC, name)) as a, open(tmp_path / name) as b:
             assert a.read() == b.read(), f"{name} is stale: run gen_mixcols.py"
@@ -49,6 +50,16 @@ def test_every_length_has_a_launchable_plan():
             assert T * nc <= 1024 and 1 <= minb <= 8
             pitch = nc + 1 if nc >= 16 else nc
             assert max(L * pitch, nc * (L | 1)) * es <= 200 * 1024
+
+
+def test_rows_plans_fit_their_launch_limits():
+    g = _gen()
+    for L in [L for L in range(48, 1025) if g.smooth7(L)]:
+        for es in (8, 16):
+            sched, nc, minb, tt = g.rows_plan(L, es)
+            T = tt if tt else L // max(sched)
+            assert nc & (nc - 1) == 0 and 1 <= nc <= 64 and T * nc <= 1024 and minb * T * nc <= 2048
+            assert nc * (L | 1) * es <= 64 * 1024
 
 
 def _stockham(x, sched, T):

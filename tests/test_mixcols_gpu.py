@@ -117,3 +117,48 @@ def test_mixc_strided_columns(n, cols, stride):
     for c in range(cols):
         ref = np.fft.fft(x[c::stride][:n].astype(np.complex128))
         assert rel_l2(got[c::stride][:n], ref) <= tol_c2c(n, False), c
+
+
+# one-pass compiled schedules (rows mode): several whole transforms per CTA;
+# lengths with both thread layouts, the smallest and largest table lengths
+ROWS = [48, 60, 100, 120, 147, 343, 500, 756, 1000, 1024]
+
+
+@pytest.mark.parametrize("n", ROWS)
+@pytest.mark.parametrize("c128", [False, True])
+def test_mixr_one_pass(n, c128):
+    dt = np.complex128 if c128 else np.complex64
+    prec = algofft.COMPLEX128 if c128 else algofft.COMPLEX64
+    count = 37  # not a multiple of the transforms per CTA: a partial last CTA
+    x = seeded_complex(n * count, seed=n, dtype=dt)
+    tok = f"gpu-sm100-mixr-n{n}"
+    if n & (n - 1):  # powers of two keep their own single-pass kernel (the token still builds)
+        assert tok in algofft.Variants(n, prec)
+        with algofft.Plan(n, prec) as p:
+            assert p.Algorithm() == tok
+    with algofft.Plan(n, prec, variant=tok) as p:
+        y = _run(p, x, count)
+        back = _run(p, y, count, inverse=True)
+        inplace = _run(p, x, count, inplace=True)
+    ref = np.fft.fft(x.astype(np.complex128).reshape(count, n), axis=1).ravel()
+    assert rel_l2(y, ref) <= tol_c2c(n, c128)
+    assert rel_l2(back, x) <= 2 * tol_c2c(n, c128)
+    np.testing.assert_array_equal(y, inplace)
+
+
+def test_mixr_batch_distance():
+    """Transforms dist > n apart: each read and written at its own offset,
+    the gaps left alone."""
+    import torch
+    n, count, dist = 360, 9, 360 + 13
+    x = seeded_complex(dist * count, seed=4)
+    with algofft.Plan(n, variant="gpu-sm100-mixr-n360") as p:
+        src = torch.from_numpy(x).cuda()
+        dst = torch.zeros_like(src)
+        p.StridedBatch(dst, src, count, 1, dist)
+        torch.cuda.synchronize()
+        got = dst.cpu().numpy()
+    for b in range(count):
+        ref = np.fft.fft(x[b * dist:b * dist + n].astype(np.complex128))
+        assert rel_l2(got[b * dist:b * dist + n], ref) <= tol_c2c(n, False)
+        assert not np.any(got[b * dist + n:(b + 1) * dist])

@@ -62,5 +62,6 @@ def test_variants_listed_without_device():
     v = algofft.Variants(1 << 20)
     assert any(t.startswith("gpu-sm100-tp-1024x1024-") for t in v)
     # 7-smooth lengths: runtime-radix schedules against Bluestein
-    assert algofft.Variants(1000) == ["gpu-sm100-mixed-n1000", "gpu-sm100-mixed2-25x40", "gpu-sm100-bluestein-n1000"]
+    assert algofft.Variants(1000) == ["gpu-sm100-mixed-n1000", "gpu-sm100-mixr-n1000", "gpu-sm100-mixed2-25x40",
+                                      "gpu-sm100-bluestein-n1000"]
     assert algofft.Variants(1009) == []  # a prime: Bluestein is the only schedule
