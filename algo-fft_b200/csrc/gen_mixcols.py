@@ -103,6 +103,12 @@ def plan(L, es, extra=0):
     return sched, nc, minb(L, sched, nc, es, T, extra), T if wide else 0
 
 
+def rows_pitch(L, sched):
+    """Shared-memory elements per transform in rows mode (MixTileRows::LP)."""
+    r0 = sched[0]
+    return (L + (L - 1) // r0 + 1 if r0 % 2 == 0 else L) | 1
+
+
 def rows_plan(L, es):
     """Rows mode: the column schedule and thread layout; transforms per CTA
     (a power of two) as many as keep the CTA within 512 threads and 64 KB of
@@ -110,13 +116,14 @@ def rows_plan(L, es):
     2048 threads and 200 KB per SM."""
     sched, _, _, tt = plan(L, es)
     T = tt if tt else L // max(sched)
+    lp = rows_pitch(L, sched)
     nc = 1
-    while nc < 64 and T * nc * 2 <= 512 and 2 * nc * (L | 1) * es <= 64 * 1024:
+    while nc < 64 and T * nc * 2 <= 512 and 2 * nc * lp * es <= 64 * 1024:
         nc *= 2
     tpb = T * nc
     tpbw = -(-tpb // 32) * 32
     regs = int(2 * (es // 8) * vmax(L, sched, T) * (1.0 if es == 8 else 1.3)) + 40
-    smem = nc * (L | 1) * es
+    smem = nc * lp * es
     k = 1
     while (k < 8 and 65536 // ((k + 1) * tpbw) >= regs and (k + 1) * tpb <= 2048
            and (k + 1) * smem <= 200 * 1024):

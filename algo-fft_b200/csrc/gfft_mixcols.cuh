@@ -57,6 +57,8 @@ struct MixSched {
 // threads per column (0: L / max radix).
 // Shared memory: element (row, c) at row * PITCH + c, PITCH = NC + 1 (odd)
 // for NC >= 16, else rows of NC with the column XOR-swizzled by the row.
+// (Skipping a row every R0 rows for even first radices, as rows mode does,
+// measured 2% slower here, up to 20% for some complex128 lengths.)
 // Pass 1's transposed result: column c at c * LP, LP = L rounded up to odd,
 // so the NC columns a warp writes at once fall in distinct banks.
 template <typename SC, int NC, int TT = 0>
@@ -309,15 +311,19 @@ namespace gfft {
 
 // Rows mode: NC whole contiguous transforms of length L per CTA, thread t of
 // transform c at tid = c * T + t (consecutive threads walk one transform, so
-// every load and store is coalesced); transform c's elements at c * LP + row
-// in shared memory (LP odd: a warp's consecutive rows fall in distinct banks).
+// every load and store is coalesced); transform c's elements contiguous in
+// shared memory, LP apart (odd).  The first stage writes its outputs R0 (its
+// radix) apart across consecutive threads; an even R0 would put a half-warp
+// in a few banks, so rows then get one element of padding every R0 rows.
 template <typename SC, int NC, int TT = 0>
 struct MixTileRows {
   static constexpr int L = SC::L;
   static constexpr int T = TT > 0 ? TT : L / SC::rmax();
   static constexpr int TPB = T * NC;
   static_assert(TPB <= 1024, "tile needs more than 1024 threads");
-  static constexpr int LP = L | 1;
+  static constexpr int R0 = SC::radix(0);
+  static constexpr bool PAD = R0 % 2 == 0;
+  static constexpr int LP = (PAD ? L + (L - 1) / R0 + 1 : L) | 1;
   static constexpr int ELEMS = NC * LP;
   __host__ __device__ static constexpr int q_at(int s) { return (L / SC::radix(s) + T - 1) / T; }
   __host__ __device__ static constexpr int vmax() {
@@ -325,7 +331,10 @@ struct MixTileRows {
     for (int s = 0; s < SC::NS; ++s) m = q_at(s) * SC::radix(s) > m ? q_at(s) * SC::radix(s) : m;
     return m;
   }
-  __device__ static __forceinline__ int phys(int row, int c) { return c * LP + row; }
+  __device__ static __forceinline__ int phys(int row, int c) {
+    if constexpr (PAD) return c * LP + row + row / R0;
+    else return c * LP + row;
+  }
 };
 
 struct MixRowsParams {

@@ -42,8 +42,8 @@ void mix_rows_part_0(std::vector<MixRowsEntry>& v) {
                               MixCfg<MixSched<24, 18>, 8, 2, 24>>());  // 432
   v.push_back(mix_rows_entry<MixCfg<MixSched<24, 20>, 16, 1, 24>,
                               MixCfg<MixSched<24, 20>, 8, 2, 24>>());  // 480
-  v.push_back(mix_rows_entry<MixCfg<MixSched<24, 21>, 16, 1, 24>,
-                              MixCfg<MixSched<24, 21>, 8, 2, 24>>());  // 504
+  v.push_back(mix_rows_entry<MixCfg<MixSched<24, 21>, 8, 3, 24>,
+                              MixCfg<MixSched<24, 21>, 4, 4, 24>>());  // 504
   v.push_back(mix_rows_entry<MixCfg<MixSched<28, 20>, 8, 3, 0>,
                               MixCfg<MixSched<28, 20>, 4, 2, 28>>());  // 560
   v.push_back(mix_rows_entry<MixCfg<MixSched<25, 24>, 8, 3, 25>,
@@ -60,8 +60,8 @@ void mix_rows_part_0(std::vector<MixRowsEntry>& v) {
                               MixCfg<MixSched<35, 25>, 4, 1, 0>>());  // 875
   v.push_back(mix_rows_entry<MixCfg<MixSched<35, 27>, 8, 2, 35>,
                               MixCfg<MixSched<35, 27>, 4, 1, 0>>());  // 945
-  v.push_back(mix_rows_entry<MixCfg<MixSched<40, 25>, 8, 2, 0>,
-                              MixCfg<MixSched<40, 25>, 4, 1, 0>>());  // 1000
+  v.push_back(mix_rows_entry<MixCfg<MixSched<40, 25>, 4, 3, 0>,
+                              MixCfg<MixSched<40, 25>, 2, 3, 0>>());  // 1000
 }
 
 }  // namespace gfft

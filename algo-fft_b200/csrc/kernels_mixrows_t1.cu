@@ -7,7 +7,7 @@ void mix_rows_part_1(std::vector<MixRowsEntry>& v) {
   v.push_back(mix_rows_entry<MixCfg<MixSched<7, 7>, 64, 2, 0>,
                               MixCfg<MixSched<7, 7>, 64, 1, 0>>());  // 49
   v.push_back(mix_rows_entry<MixCfg<MixSched<10, 6>, 64, 2, 0>,
-                              MixCfg<MixSched<10, 6>, 64, 1, 0>>());  // 60
+                              MixCfg<MixSched<10, 6>, 32, 3, 0>>());  // 60
   v.push_back(mix_rows_entry<MixCfg<MixSched<9, 8>, 32, 3, 9>,
                               MixCfg<MixSched<9, 8>, 32, 2, 9>>());  // 72
   v.push_back(mix_rows_entry<MixCfg<MixSched<12, 7>, 64, 2, 0>,
@@ -15,7 +15,7 @@ void mix_rows_part_1(std::vector<MixRowsEntry>& v) {
   v.push_back(mix_rows_entry<MixCfg<MixSched<10, 10>, 32, 3, 0>,
                               MixCfg<MixSched<10, 10>, 32, 2, 0>>());  // 100
   v.push_back(mix_rows_entry<MixCfg<MixSched<12, 10>, 32, 2, 12>,
-                              MixCfg<MixSched<12, 10>, 32, 1, 12>>());  // 120
+                              MixCfg<MixSched<12, 10>, 16, 3, 12>>());  // 120
   v.push_back(mix_rows_entry<MixCfg<MixSched<15, 9>, 32, 2, 0>,
                               MixCfg<MixSched<15, 9>, 16, 2, 15>>());  // 135
   v.push_back(mix_rows_entry<MixCfg<MixSched<15, 10>, 32, 2, 0>,
@@ -60,8 +60,8 @@ void mix_rows_part_1(std::vector<MixRowsEntry>& v) {
                               MixCfg<MixSched<42, 21>, 4, 2, 0>>());  // 882
   v.push_back(mix_rows_entry<MixCfg<MixSched<32, 30>, 8, 2, 32>,
                               MixCfg<MixSched<32, 30>, 4, 2, 32>>());  // 960
-  v.push_back(mix_rows_entry<MixCfg<MixSched<36, 28>, 8, 2, 36>,
-                              MixCfg<MixSched<36, 28>, 4, 1, 0>>());  // 1008
+  v.push_back(mix_rows_entry<MixCfg<MixSched<36, 28>, 4, 3, 36>,
+                              MixCfg<MixSched<36, 28>, 2, 3, 0>>());  // 1008
 }
 
 }  // namespace gfft

@@ -15,7 +15,7 @@ void mix_rows_part_3(std::vector<MixRowsEntry>& v) {
   v.push_back(mix_rows_entry<MixCfg<MixSched<12, 9>, 32, 2, 12>,
                               MixCfg<MixSched<12, 9>, 32, 1, 12>>());  // 108
   v.push_back(mix_rows_entry<MixCfg<MixSched<14, 9>, 32, 2, 0>,
-                              MixCfg<MixSched<14, 9>, 32, 1, 14>>());  // 126
+                              MixCfg<MixSched<14, 9>, 16, 2, 14>>());  // 126
   v.push_back(mix_rows_entry<MixCfg<MixSched<12, 12>, 32, 2, 0>,
                               MixCfg<MixSched<12, 12>, 16, 3, 0>>());  // 144
   v.push_back(mix_rows_entry<MixCfg<MixSched<18, 9>, 32, 2, 0>,
@@ -26,8 +26,8 @@ void mix_rows_part_3(std::vector<MixRowsEntry>& v) {
                               MixCfg<MixSched<15, 14>, 16, 2, 15>>());  // 210
   v.push_back(mix_rows_entry<MixCfg<MixSched<16, 15>, 32, 1, 16>,
                               MixCfg<MixSched<16, 15>, 16, 2, 16>>());  // 240
-  v.push_back(mix_rows_entry<MixCfg<MixSched<18, 14>, 32, 1, 0>,
-                              MixCfg<MixSched<18, 14>, 16, 1, 18>>());  // 252
+  v.push_back(mix_rows_entry<MixCfg<MixSched<18, 14>, 16, 3, 0>,
+                              MixCfg<MixSched<18, 14>, 8, 3, 18>>());  // 252
   v.push_back(mix_rows_entry<MixCfg<MixSched<18, 16>, 16, 2, 18>,
                               MixCfg<MixSched<18, 16>, 8, 3, 18>>());  // 288
   v.push_back(mix_rows_entry<MixCfg<MixSched<20, 16>, 16, 2, 0>,

@@ -59,7 +59,7 @@ def test_rows_plans_fit_their_launch_limits():
             sched, nc, minb, tt = g.rows_plan(L, es)
             T = tt if tt else L // max(sched)
             assert nc & (nc - 1) == 0 and 1 <= nc <= 64 and T * nc <= 1024 and minb * T * nc <= 2048
-            assert nc * (L | 1) * es <= 64 * 1024
+            assert nc * g.rows_pitch(L, sched) * es <= 64 * 1024
 
 
 def _stockham(x, sched, T):
