@@ -1,9 +1,11 @@
 """Writes kernels_mixcols_t0.cu .. kernels_mixcols_t7.cu: the compiled
 mixed-radix column tiles (gfft_mixcols.cuh) of every 7-smooth column length
 48 <= L <= 1024, spread over eight files so nvcc builds them in parallel; and
-kernels_mixrows_t0.cu .. kernels_mixrows_t3.cu: the same schedules in rows
+kernels_mixrows_t0.cu .. kernels_mixrows_t7.cu: the same schedules in rows
 mode (k_mix_rows: whole contiguous transforms of every table length, several
-per CTA, the single-pass plans of those lengths); and
+per CTA, the single-pass plans of those lengths), plus three-stage schedules
+for the 7-smooth lengths 1025..12288 that are not powers of two (complex128
+up to 6144, the shared memory one transform can have); and
 kernels_mixbs_t0.cu .. kernels_mixbs_t2.cu: the Bluestein chain's passes
 (gfft_mixbs.cuh) for the column lengths its FFT lengths M = M1 x M2 are built
 from (BS_LENGTHS: the multiples of 16 up to 512, whose products come within
@@ -33,7 +35,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 PARTS = 8
 BS_PARTS = 3
-ROW_PARTS = 4
+ROW_PARTS = 8
+ROWS3_MAX = {8: 12288, 16: 6144}  # longest three-stage rows length per element size
 
 
 def smooth7(n):
@@ -103,6 +106,28 @@ def plan(L, es, extra=0):
     return sched, nc, minb(L, sched, nc, es, T, extra), T if wide else 0
 
 
+def schedule3(L):
+    """Three stages L = a * b * c, a >= b >= c, the largest radix as small as
+    it can be, then the smallest as large."""
+    best = None
+    for a in range(2, 65):
+        if L % a or not radix_ok(a):
+            continue
+        for b in range(2, a + 1):
+            if (L // a) % b or not radix_ok(b):
+                continue
+            c = L // a // b
+            if 2 <= c <= b and radix_ok(c) and (best is None or (a, -c) < best[0]):
+                best = ((a, -c), (a, b, c))
+    if best is None:
+        raise ValueError(f"no three-stage schedule for {L}")
+    return best[1]
+
+
+def rows3_lengths(es):
+    return [L for L in range(1025, ROWS3_MAX[es] + 1) if smooth7(L) and L & (L - 1)]
+
+
 def rows_pitch(L, sched):
     """Shared-memory elements per transform in rows mode (MixTileRows::LP)."""
     r0 = sched[0]
@@ -114,8 +139,12 @@ def rows_plan(L, es):
     (a power of two) as many as keep the CTA within 512 threads and 64 KB of
     shared memory; resident CTAs per SM by the same register estimate, up to
     2048 threads and 200 KB per SM."""
-    sched, _, _, tt = plan(L, es)
+    if L <= 1024:
+        sched, _, _, tt = plan(L, es)
+    else:
+        sched, tt = schedule3(L), 0
     T = tt if tt else L // max(sched)
+    assert T <= 1024, (L, sched)
     lp = rows_pitch(L, sched)
     nc = 1
     while nc < 64 and T * nc * 2 <= 512 and 2 * nc * lp * es <= 64 * 1024:
@@ -161,8 +190,12 @@ def main(out=HERE):
                      "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
                      f"void mix_part_{k}(std::vector<MixEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
     rparts = [[] for _ in range(ROW_PARTS)]
-    for i, L in enumerate(lengths):
-        rparts[i % ROW_PARTS].append(f"  v.push_back(mix_rows_entry<{rows_cfg(L, 8)},\n                              {rows_cfg(L, 16)}>());  // {L}\n")
+    for i, L in enumerate(lengths + rows3_lengths(8)):
+        if L <= 1024 or L in rows3_lengths(16):
+            e = f"  v.push_back(mix_rows_entry<{rows_cfg(L, 8)},\n                              {rows_cfg(L, 16)}>());  // {L}\n"
+        else:
+            e = f"  v.push_back(mix_rows_entry64<{rows_cfg(L, 8)}>());  // {L}\n"
+        rparts[i % ROW_PARTS].append(e)
     for k, body in enumerate(rparts):
         with open(os.path.join(out, f"kernels_mixrows_t{k}.cu"), "w") as fh:
             fh.write("// Generated by gen_mixcols.py; do not edit.\n"
@@ -176,7 +209,7 @@ def main(out=HERE):
             fh.write("// Generated by gen_mixcols.py; do not edit.\n"
                      "#include \"kernels_mixcols.cuh\"\n\nnamespace gfft {\n\n"
                      f"void mix_bs_part_{k}(std::vector<MixBsEntry>& v) {{\n" + "".join(body) + "}\n\n}  // namespace gfft\n")
-    print(len(lengths), "lengths,", len(bs_lengths()), "Bluestein lengths")
+    print(len(lengths), "lengths,", len(rows3_lengths(8)), "three-stage rows lengths,", len(bs_lengths()), "Bluestein lengths")
 
 
 if __name__ == "__main__":

@@ -123,9 +123,11 @@ cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams 
 // 0 when none), and one of its passes (BSK_IN / BSK_FILT / BSK_OUT) over
 // `count` transforms, or `count` CTAs in item mode.
 struct MixBsParams;
-// Whole contiguous transforms of a compiled column length (rows mode).
+// Whole contiguous transforms of a compiled length (rows mode: every
+// 7-smooth length 48..1024, and the non-powers of two up to 12288 for
+// complex64, 6144 for complex128).
 struct MixRowsParams;
-bool mix_rows_supported(int64_t L);
+bool mix_rows_supported(int prec, int64_t L);
 cudaError_t exec_mix_rows(int prec, int dir, int64_t L, const MixRowsParams& p, cudaStream_t st);
 int64_t bs_mixed_length(int64_t n, int64_t* m1);
 int mix_bs_width(int prec, int64_t L);

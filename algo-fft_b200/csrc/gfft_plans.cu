@@ -189,7 +189,7 @@ gfft_status init_generic(PlanCore* c, bool mixr) {
   GenSched s;
   const size_t es = elem_bytes(c->prec);
   if (mixr) {
-    if (!mix_rows_supported(c->n)) return GFFT_ERR_NOT_IMPLEMENTED;
+    if (!mix_rows_supported(c->prec, c->n)) return GFFT_ERR_NOT_IMPLEMENTED;
     gfft_status st = make_twiddles(c->prec, c->n, &c->tw, 0);
     if (st != GFFT_OK) return st;
     GFFT_CUDA(cudaStreamSynchronize(0));
@@ -241,7 +241,7 @@ std::vector<std::string> mixed_tokens(int prec, int64_t n) {
   const size_t es = elem_bytes(prec);
   GenSched s, s1, s2;
   if (make_sched(n, &s) && size_t(s.stride) * es <= size_t(kSmemBudget)) v.push_back("gpu-sm100-mixed-n" + std::to_string(n));
-  if (mix_rows_supported(n)) v.push_back("gpu-sm100-mixr-n" + std::to_string(n));
+  if (mix_rows_supported(prec, n)) v.push_back("gpu-sm100-mixr-n" + std::to_string(n));
   const int64_t n1 = gen_split(n), n2 = n / n1;
   const int want = prec == kC64 ? 16 : 8;
   if (n1 >= 2 && make_col_sched(n1, es, want, &s1) && make_col_sched(n2, es, want, &s2))

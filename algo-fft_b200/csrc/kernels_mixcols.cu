@@ -19,6 +19,10 @@ void mix_rows_part_0(std::vector<MixRowsEntry>& v);
 void mix_rows_part_1(std::vector<MixRowsEntry>& v);
 void mix_rows_part_2(std::vector<MixRowsEntry>& v);
 void mix_rows_part_3(std::vector<MixRowsEntry>& v);
+void mix_rows_part_4(std::vector<MixRowsEntry>& v);
+void mix_rows_part_5(std::vector<MixRowsEntry>& v);
+void mix_rows_part_6(std::vector<MixRowsEntry>& v);
+void mix_rows_part_7(std::vector<MixRowsEntry>& v);
 void mix_bs_part_0(std::vector<MixBsEntry>& v);
 void mix_bs_part_1(std::vector<MixBsEntry>& v);
 void mix_bs_part_2(std::vector<MixBsEntry>& v);
@@ -46,7 +50,9 @@ const MixEntry* find(int64_t L) {
 const std::vector<MixRowsEntry>& rows_table() {
   static const std::vector<MixRowsEntry> t = [] {
     std::vector<MixRowsEntry> v;
-    for (auto part : {&mix_rows_part_0, &mix_rows_part_1, &mix_rows_part_2, &mix_rows_part_3}) part(v);
+    for (auto part : {&mix_rows_part_0, &mix_rows_part_1, &mix_rows_part_2, &mix_rows_part_3, &mix_rows_part_4,
+                      &mix_rows_part_5, &mix_rows_part_6, &mix_rows_part_7})
+      part(v);
     std::sort(v.begin(), v.end(), [](const MixRowsEntry& a, const MixRowsEntry& b) { return a.L < b.L; });
     return v;
   }();
@@ -96,12 +102,14 @@ int64_t bs_mixed_length(int64_t n, int64_t* m1) {
   return best;
 }
 
-bool mix_rows_supported(int64_t L) { return rows_find(L) != nullptr; }
+bool mix_rows_supported(int prec, int64_t L) {
+  const MixRowsEntry* e = rows_find(L);
+  return e && (prec == kC64 || prec == kC128) && e->fn[prec][0];
+}
 
 cudaError_t exec_mix_rows(int prec, int dir, int64_t L, const MixRowsParams& p, cudaStream_t st) {
-  const MixRowsEntry* e = rows_find(L);
-  if (!e || (prec != kC64 && prec != kC128)) return cudaErrorNotSupported;
-  return e->fn[prec][dir < 0 ? 0 : 1](p, st);
+  if (!mix_rows_supported(prec, L)) return cudaErrorNotSupported;
+  return rows_find(L)->fn[prec][dir < 0 ? 0 : 1](p, st);
 }
 
 int mix_bs_width(int prec, int64_t L) {

@@ -115,7 +115,7 @@ using MixRowsFn = cudaError_t (*)(const MixRowsParams&, cudaStream_t);
 struct MixRowsEntry {
   int L;
   int nc[2];           // transforms per CTA per precision
-  MixRowsFn fn[2][2];  // [prec][dir < 0 ? 0 : 1]
+  MixRowsFn fn[2][2];  // [prec][dir < 0 ? 0 : 1]; null where a precision has no schedule
 };
 
 template <typename C, typename CFG, int DIR>
@@ -133,6 +133,17 @@ cudaError_t launch_mix_rows(const MixRowsParams& p, cudaStream_t st) {
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   kern<<<unsigned(blocks), TL::TPB, smem, st>>>(p);
   return cudaGetLastError();
+}
+
+// Complex64 only (lengths beyond a complex128 transform's shared memory).
+template <typename F>
+MixRowsEntry mix_rows_entry64() {
+  MixRowsEntry e{};
+  e.L = F::Sched::L;
+  e.nc[kC64] = F::nc;
+  e.fn[kC64][0] = &launch_mix_rows<float2, F, -1>;
+  e.fn[kC64][1] = &launch_mix_rows<float2, F, +1>;
+  return e;
 }
 
 template <typename F, typename D>

@@ -120,16 +120,20 @@ def test_mixc_strided_columns(n, cols, stride):
 
 
 # one-pass compiled schedules (rows mode): several whole transforms per CTA;
-# lengths with both thread layouts, the smallest and largest table lengths
-ROWS = [48, 60, 100, 120, 147, 343, 500, 756, 1000, 1024]
+# lengths with both thread layouts, the smallest and largest table lengths,
+# three-stage schedules (1080 = 12 x 10 x 9 .. 12000 = 25 x 24 x 20;
+# complex128 up to 6144)
+ROWS = [48, 60, 100, 120, 147, 343, 500, 756, 1000, 1024, 1080, 2000, 6000, 6561, 10000, 12000]
 
 
 @pytest.mark.parametrize("n", ROWS)
 @pytest.mark.parametrize("c128", [False, True])
 def test_mixr_one_pass(n, c128):
+    if c128 and n > 6144:
+        pytest.skip("complex128 three-stage rows stop at 6144")
     dt = np.complex128 if c128 else np.complex64
     prec = algofft.COMPLEX128 if c128 else algofft.COMPLEX64
-    count = 37  # not a multiple of the transforms per CTA: a partial last CTA
+    count = 37 if n <= 2000 else 5  # not a multiple of the transforms per CTA: a partial last CTA
     x = seeded_complex(n * count, seed=n, dtype=dt)
     tok = f"gpu-sm100-mixr-n{n}"
     if n & (n - 1):  # powers of two keep their own single-pass kernel (the token still builds)
