@@ -31,7 +31,7 @@ import time
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import ErrInvalidArgument, check, lib
 from .plan import COMPLEX64, COMPLEX128, Plan, PlanOptions
 from .wisdom import ClearWisdom, ExportWisdomToString, ImportWisdomFromString, Variants
 
@@ -218,11 +218,17 @@ def load_records(path: str = DEFAULT_DATA) -> list[dict]:
 
 def design(records: list[dict]):
     """X (rows x D raw features), y (log ns per element), owner shape index,
-    and the token of each row."""
+    and the token of each row.  Variants without features (the L2-pipelined
+    two-pass, an autotuner candidate only) are left out, as plan creation
+    leaves them out of the model's candidates."""
     X, y, owner, toks = [], [], [], []
     for i, r in enumerate(records):
         for tok, ms in r["times"].items():
-            X.append(features(r["prec"], r["n"], r["batch"], 1, r["real"], tok))
+            try:
+                x = features(r["prec"], r["n"], r["batch"], 1, r["real"], tok)
+            except ErrInvalidArgument:
+                continue
+            X.append(x)
             y.append(math.log(ms * 1e6 / (r["n"] * r["batch"])))
             owner.append(i)
             toks.append(tok)

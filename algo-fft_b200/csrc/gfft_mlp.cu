@@ -286,11 +286,26 @@ static bool plan_features(int prec, int64_t n, int64_t batch, int64_t stride, in
     f[12] = 1.f;
     f[14] = 1.f;
     f[15] = float(std::log2(double(l1)));
+  } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixc-%lldx%lld", &l1, &l2) == 2) {
+    f[12] = 1.f;  // the compiled mixed-radix four-step (marker 3)
+    f[14] = 3.f;
+    f[15] = float(std::log2(double(l1)));
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixed-n%lld", &ln) == 1) {
     f[12] = 1.f;
+  } else if (std::sscanf(tok.c_str(), "gpu-sm100-mixr-n%lld", &ln) == 1) {
+    f[12] = 1.f;  // the compiled single pass (marker 2)
+    f[14] = 2.f;
   } else if (std::sscanf(tok.c_str(), "gpu-sm100-bluestein-n%lld", &ln) == 1) {
+    // FFT length: NextPow2(2n - 1), or the mixed length for "-mx" (marker 1)
     int64_t M = 1;
     while (M < 2 * n - 1) M <<= 1;
+    const std::string mx = "gpu-sm100-bluestein-n" + std::to_string(n) + "-mx";
+    int64_t m1 = 0;
+    const int64_t x = tok.compare(0, mx.size(), mx) == 0 ? bs_mixed_choice(n, &m1) : 0;
+    if (x > 0) {
+      M = x;
+      f[14] = 1.f;
+    }
     f[13] = 1.f;
     f[15] = float(std::log2(double(M)));
   } else {
@@ -392,41 +407,12 @@ bool learned_choose(int prec, int64_t n, const PlanHint& hint, std::string* toke
   std::lock_guard<std::mutex> g(M.mu);
   model_try_default();
   if (!M.loaded) return false;
-  // Variant families added after the model was trained are scored as the
-  // family they refine: the compiled mixed-radix four-step ("-mixc-AxB") with
-  // the features of the runtime-radix split AxB, replacing the runtime
-  // four-step it outruns (2-3x at every length measured), the compiled
-  // single pass ("-mixr-nN") likewise for the runtime one; Bluestein's two FFT
-  // lengths ("-mx" / "-p2") as one Bluestein candidate whose length the
-  // plan's own rule picks.  Candidates of any other unknown kind are left out.
-  const std::vector<std::string> cands = variant_tokens(prec, n);
-  bool has_mixc = false, has_mixr = false;
-  for (const std::string& t : cands) {
-    has_mixc |= t.find("-mixc-") != std::string::npos;
-    has_mixr |= t.find("-mixr-") != std::string::npos;
-  }
-  const std::string bs_plain = "gpu-sm100-bluestein-n" + std::to_string(n);
-  bool bs_added = false;
+  // candidates of a kind the model has no features for are left out
   std::vector<std::string> toks;
   std::vector<float> xs;
-  for (const std::string& t0 : cands) {
-    std::string t = t0, ft = t0;
-    const size_t mc = t0.find("-mixc-");
-    const size_t mr = t0.find("-mixr-");
-    if (mc != std::string::npos) {
-      ft = "gpu-sm100-mixed2-" + t0.substr(mc + 6);
-    } else if (mr != std::string::npos) {
-      ft = "gpu-sm100-mixed-" + t0.substr(mr + 6);
-    } else if ((has_mixc && t0.rfind("gpu-sm100-mixed2-", 0) == 0) ||
-               (has_mixr && t0.rfind("gpu-sm100-mixed-n", 0) == 0)) {
-      continue;
-    } else if (t0 == bs_plain + "-mx" || t0 == bs_plain + "-p2") {
-      if (bs_added) continue;
-      bs_added = true;
-      t = ft = bs_plain;
-    }
+  for (const std::string& t : variant_tokens(prec, n)) {
     float f[D];
-    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, ft, f)) continue;
+    if (!plan_features(prec, n, hint.batch, hint.stride, hint.real, t, f)) continue;
     for (int d = 0; d < D; ++d) xs.push_back((f[d] - M.norm[d]) / M.norm[D + d]);
     toks.push_back(t);
   }

@@ -394,11 +394,7 @@ GFFT_API gfft_status gfft_planner_set_model(const float* params, const float* no
 GFFT_API gfft_status gfft_planner_load_model(const char* path);
 GFFT_API int32_t gfft_planner_has_model(void);
 /* The model's pick among gfft_plan_variants(n) for a shape (one inference
- * launch on the current device).  Families the model was not trained on are
- * scored as the family they refine: a "-mixc-AxB" variant as the runtime
- * split "-mixed2-AxB" it replaces, Bluestein's "-mx" / "-p2" pair as the
- * plain Bluestein token (its FFT length then chosen by the plan's rule),
- * which is what the pick returns in that case. */
+ * launch on the current device). */
 GFFT_API gfft_status gfft_planner_choose(int32_t precision, int64_t n, int64_t batch, int64_t stride, int32_t real,
                                          char* token, size_t cap);
 

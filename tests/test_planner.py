@@ -34,6 +34,16 @@ def test_sizes_and_feature_map():
     assert list(f[6:10]) == [6, 1, 3, 1] and list(f[10:14]) == [0, 1, 0, 0] and list(f[14:]) == [4, 13]
     f = P.features(0, 1009, 4, 1, 0, "gpu-sm100-bluestein-n1009")
     assert f[5] == pytest.approx(np.log2(1009)) and f[13] == 1 and f[15] == 11
+    # compiled mixed-radix families: markers 2 (single pass) and 3 (four-step)
+    f = P.features(0, 1000, 4, 1, 0, "gpu-sm100-mixr-n1000")
+    assert list(f[10:14]) == [0, 0, 1, 0] and f[14] == 2 and f[15] == 0
+    f = P.features(0, 50421, 4, 1, 0, "gpu-sm100-mixc-147x343")
+    assert list(f[10:14]) == [0, 0, 1, 0] and f[14] == 3 and f[15] == pytest.approx(np.log2(147))
+    # Bluestein on the mixed length (marker 1) against the power of two
+    f = P.features(0, 16411, 4, 1, 0, "gpu-sm100-bluestein-n16411-mx")
+    assert f[13] == 1 and f[14] == 1 and f[15] == pytest.approx(np.log2(34560))
+    f = P.features(0, 16411, 4, 1, 0, "gpu-sm100-bluestein-n16411-p2")
+    assert f[13] == 1 and f[14] == 0 and f[15] == 16
     with pytest.raises(algofft.ErrInvalidArgument):
         P.features(0, 64, 1, 1, 0, "no-such-variant")
 
