@@ -658,7 +658,7 @@ def _convolve(dev, stream, iters, gen):
 
 
 CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "bs_mixed", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
-         "gen_cols", "mix_cols", "tp3t", "tp2", "p16384")
+         "gen_cols", "mix_cols", "mix_rows", "tp3t", "tp2", "p16384")
 
 
 def run_case(name: str, reps: int) -> int:
@@ -729,12 +729,14 @@ def run_case(name: str, reps: int) -> int:
         p = algofft.Plan(n, variant=f"gpu-sm100-tc16-n{n}")
         close.append(p)
         fn = lambda: p.ForwardBatch(y, x, count)  # noqa: E731
-    elif name in ("l2p", "tp3t", "gen_cols", "mix_cols", "tp2", "p16384"):
+    elif name in ("l2p", "tp3t", "gen_cols", "mix_cols", "mix_rows", "tp2", "p16384"):
         # L2-pipelined 2^20 (16 transforms, 16 MB groups), TMA three-pass 2^23 (4), runtime two-pass 50421
-        # (160), compiled mixed-radix two-pass 50421 (640: 256 MiB), the default plan of 2^20 (split two-pass, 16),
+        # (160), compiled mixed-radix two-pass 50421 (640: 256 MiB), compiled three-stage single pass 6000
+        # (5592: 256 MiB), the default plan of 2^20 (split two-pass, 16),
         # single pass 16384 (4096)
         n, count, tok = {"l2p": (1 << 20, 16, "-l2p-1024x1024-c8x8-e16x16-s3-g16"), "tp3t": (1 << 23, 4, "-tp3t-"),
                          "gen_cols": (50421, 160, "-mixed2-"), "mix_cols": (50421, 640, "-mixc-"),
+                         "mix_rows": (6000, 5592, "-mixr-"),
                          "tp2": (1 << 20, 16, None),
                          "p16384": (16384, 4096, None)}[name]
         x = cplx(n * count)
