@@ -1,10 +1,13 @@
 // Bluestein chain for FFT lengths M = 2^15..2^20 (two-pass FFT_M) with the
 // element-wise steps fused into the passes: the chirp multiply and zero pad
-// into the loads of the forward FFT's first pass, the filter product into
-// the stores of its second pass, the chirp multiply (with 1/M, and 1/n for
-// the inverse) into the stores of the inverse FFT's second pass, which
-// writes only the n outputs.  Four launches and about 6 M + 2 n element
-// transfers per transform, where the separate chain (plan_bluestein.go:7-58,
+// into the loads of the forward FFT's first pass (BS_FWD1); the forward
+// FFT's second pass, the filter product and the inverse FFT's first pass in
+// one tile (BS_MID: the inverse FFT splits M the other way, N2 x N1, so
+// that column k1 of the forward output is column k1 of its input); the
+// chirp multiply (with 1/M, and 1/n for the inverse) in the stores of the
+// inverse FFT's second pass (BS_INV2 of the transposed split), which writes
+// only the n outputs.  Three launches and about 4 M + 2 n element transfers
+// per transform, where the separate chain (plan_bluestein.go:7-58,
 // internal/kernels/bluestein.go:20-77: pad, FFT, product, IFFT, chirp) moves
 // about 13 M.
 //
@@ -42,22 +45,6 @@ struct BsChirpIn {
   __device__ __forceinline__ C load(int row, int c) const {
     const int64_t m = int64_t(row) * n2 + col0 + c;
     return m < n ? cmul(ld_stream(x + m), chirp_of<UDIR>(w, m)) : C{0, 0};
-  }
-};
-
-// spectrum times the filter, k = col0 + c + N1 * row, kept in L2 for the
-// inverse FFT that reads it next
-template <typename C, int UDIR>
-struct BsFilterOut {
-  C* y;  // this transform's work row
-  const C* f;
-  int64_t n1, col0, m;
-  __device__ __forceinline__ void store(int row, int c, C v) const {
-    const int64_t k = col0 + c + n1 * int64_t(row);
-    C fk;
-    if constexpr (UDIR > 0) fk = cconj(__ldg(f + ((m - k) & (m - 1))));
-    else fk = __ldg(f + k);
-    __stcg(y + k, cmul(v, fk));
   }
 };
 
@@ -129,7 +116,7 @@ struct ItemOut {
   __device__ __forceinline__ void store(int row, int c, C v) const { st_stream(y + col0 + c + n1 * int64_t(row), v); }
 };
 
-enum { BS_FWD1 = 0, BS_FWD2 = 1, BS_INV2 = 2, PL_1 = 3, PL_2 = 4 };
+enum { BS_FWD1 = 0, BS_MID = 1, BS_INV2 = 2, PL_1 = 3, PL_2 = 4 };
 
 template <typename C, int N1, int EPT1, int NC1, int N2, int EPT2, int NC2, int KIND, int UDIR>
 __global__ void __launch_bounds__(TwoPass<C, N1, EPT1, NC1, N2, EPT2, NC2, -1>::TPB,
@@ -183,6 +170,38 @@ k_bs_tp(BsTpParams p, int64_t b0) {
       const int cc = e / N1, row = e % N1;
       __stcg(y + int64_t(col0 + cc) * N1 + row, sh[S1::phys(row, cc)]);
     }
+  } else if constexpr (KIND == BS_MID) {
+    // column k1 = col0 + c of the forward FFT's second pass (rows k2), the
+    // spectrum k = k1 + N1 k2 times the filter, then the same column as
+    // column b = k1 of the inverse FFT's first pass on the split N2 x N1
+    // (input index N1 a + b, a = k2), times W_M^{-b k1'}, stored as row b
+    // of the work rows (N1 rows of N2)
+    const int64_t bl = blockIdx.x / TP::TILES2;
+    const int col0 = int(blockIdx.x % TP::TILES2) * NC2;
+    const bool active = tid < S2::TPB;
+    const int c = tid % NC2, t = tid / NC2;
+    const C* y = scratch + bl * TP::N + col0;
+    const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
+    const C* tw2 = static_cast<const C*>(p.tw2);
+    col_stage<C, N2, EPT2, NC2, -1, 1, LOAD_L2, OUT_SMEM, N1, N1>(v, y, nullptr, sh, t, c, active, tw2, Re(1), p.bt,
+                                                                 0);
+    __syncthreads();
+    for (int e = tid; e < N2 * NC2; e += TP::TPB) {
+      const int row = e / NC2, cc = e % NC2;
+      const int64_t k = col0 + cc + int64_t(N1) * row;
+      C fk;
+      if constexpr (UDIR > 0) fk = cconj(__ldg(rw.f + ((TP::N - k) & (TP::N - 1))));
+      else fk = __ldg(rw.f + k);
+      sh[S2::phys(row, cc)] = cmul(sh[S2::phys(row, cc)], fk);
+    }
+    __syncthreads();
+    col_stage<C, N2, EPT2, NC2, +1, 1, LOAD_SMEM, OUT_SMEM_TWIDDLE, 0, 0>(v, nullptr, nullptr, sh, t, c, active, tw2,
+                                                                         Re(1), p.bt, int64_t(col0 + c));
+    C* wk = static_cast<C*>(p.work) + bl * TP::N;
+    for (int e = tid; e < N2 * NC2; e += TP::TPB) {
+      const int cc = e / N2, row = e % N2;
+      __stcg(wk + int64_t(col0 + cc) * N2 + row, sh[S2::phys(row, cc)]);
+    }
   } else {
     const int64_t bl = blockIdx.x / TP::TILES2;
     const int col0 = int(blockIdx.x % TP::TILES2) * NC2;
@@ -190,11 +209,7 @@ k_bs_tp(BsTpParams p, int64_t b0) {
     const int c = tid % NC2, t = tid / NC2;
     const C* y = scratch + bl * TP::N + col0;
     const BsRow<C> rw = bs_row<C, UDIR>(p, b0 + bl);
-    if constexpr (KIND == BS_FWD2) {
-      const BsFilterOut<C, UDIR> io{static_cast<C*>(p.work) + bl * TP::N, rw.f, N1, col0, TP::N};
-      col_stage<C, N2, EPT2, NC2, -1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsFilterOut<C, UDIR>>(
-          v, y, nullptr, sh, t, c, active, static_cast<const C*>(p.tw2), Re(1), p.bt, 0, 0, io);
-    } else {
+    {
       const BsChirpOut<C, UDIR> io{rw.y, rw.w, rw.n, N1, col0, Re(rw.scale)};
       col_stage<C, N2, EPT2, NC2, +1, 1, LOAD_L2, OUT_FN, N1, N1, false, BsChirpOut<C, UDIR>>(
           v, y, nullptr, sh, t, c, active, static_cast<const C*>(p.tw2), Re(p.inv_m), p.bt, 0, 0, io);
@@ -207,7 +222,7 @@ struct BsTpKernel {
   int64_t m;
   int n1;
   int tpb, smem;
-  const void* fn[11];  // fused Bluestein passes (UDIR -1, +1), this file's plain inverse first pass, item passes
+  const void* fn[10];  // fused Bluestein passes (UDIR -1, +1; the last of the transposed split), item passes
   cudaError_t (*run)(const BsTpParams& p, int udir, int64_t count, void* scratch, void* work, cudaStream_t st);
   cudaError_t (*run_plain)(const BsTpParams& p, int udir, int64_t count, void* scratch, cudaStream_t st);
 };
@@ -223,31 +238,31 @@ struct BsTpOf {
   using A = TileRule<TE, EMAX, N1>;
   using B = TileRule<TE, EMAX, N2>;
   using TP = TwoPass<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, -1>;
+  // the inverse FFT's split N2 x N1: its second pass runs columns of N1
+  using TS = TwoPass<C, N2, B::EPT, B::NC, N1, A::EPT, A::NC, -1>;
   template <int KIND, int UDIR>
   static const void* fn() {
     return reinterpret_cast<const void*>(&k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, KIND, UDIR>);
   }
   template <int UDIR>
+  static const void* fn_inv2() {
+    return reinterpret_cast<const void*>(&k_bs_tp<C, N2, B::EPT, B::NC, N1, A::EPT, A::NC, BS_INV2, UDIR>);
+  }
+  template <int UDIR>
   static cudaError_t run_dir(const BsTpParams& p, int64_t count, cudaStream_t st) {
     const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (TP::N * int64_t(sizeof(C)))));
-    TwoPassParams q{};
-    q.scratch = p.scratch;
-    q.src = p.work;
-    q.idist = TP::N;
-    q.tw1 = p.tw1;
-    q.tw2 = p.tw2;
-    q.bt = p.bt;
+    // the inverse's second pass reads the work rows with the W_N1 table
+    BsTpParams q = p;
+    q.scratch = p.work;
+    q.tw2 = p.tw1;
     for (int64_t b0 = 0; b0 < count; b0 += chunk) {
       const int64_t nb = std::min(chunk, count - b0);
       k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD1, UDIR>
           <<<unsigned(nb * TP::TILES1), TP::TPB, TP::SMEM, st>>>(p, b0);
-      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_FWD2, UDIR>
+      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_MID, UDIR>
           <<<unsigned(nb * TP::TILES2), TP::TPB, TP::SMEM, st>>>(p, b0);
-      // inverse FFT, first pass: plain, from the work rows into scratch
-      k_tp_split<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, +1, 1>
-          <<<unsigned(nb * TP::TILES1), TP::TPB, TP::SMEM, st>>>(q, 0);
-      k_bs_tp<C, N1, A::EPT, A::NC, N2, B::EPT, B::NC, BS_INV2, UDIR>
-          <<<unsigned(nb * TP::TILES2), TP::TPB, TP::SMEM, st>>>(p, b0);
+      k_bs_tp<C, N2, B::EPT, B::NC, N1, A::EPT, A::NC, BS_INV2, UDIR>
+          <<<unsigned(nb * TS::TILES2), TS::TPB, TS::SMEM, st>>>(q, b0);
       const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
@@ -293,18 +308,17 @@ void reg() {
   k.n1 = N1;
   k.tpb = O::TP::TPB;
   k.smem = O::TP::SMEM;
+  static_assert(O::TS::SMEM == O::TP::SMEM, "the transposed split needs the same shared memory");
   k.fn[0] = O::template fn<BS_FWD1, -1>();
-  k.fn[1] = O::template fn<BS_FWD2, -1>();
-  k.fn[2] = O::template fn<BS_INV2, -1>();
+  k.fn[1] = O::template fn<BS_MID, -1>();
+  k.fn[2] = O::template fn_inv2<-1>();
   k.fn[3] = O::template fn<BS_FWD1, +1>();
-  k.fn[4] = O::template fn<BS_FWD2, +1>();
-  k.fn[5] = O::template fn<BS_INV2, +1>();
-  k.fn[6] = reinterpret_cast<const void*>(
-      &k_tp_split<C, N1, O::A::EPT, O::A::NC, N2, O::B::EPT, O::B::NC, +1, 1>);
-  k.fn[7] = O::template fn<PL_1, -1>();
-  k.fn[8] = O::template fn<PL_2, -1>();
-  k.fn[9] = O::template fn<PL_1, +1>();
-  k.fn[10] = O::template fn<PL_2, +1>();
+  k.fn[4] = O::template fn<BS_MID, +1>();
+  k.fn[5] = O::template fn_inv2<+1>();
+  k.fn[6] = O::template fn<PL_1, -1>();
+  k.fn[7] = O::template fn<PL_2, -1>();
+  k.fn[8] = O::template fn<PL_1, +1>();
+  k.fn[9] = O::template fn<PL_2, +1>();
   k.run = &O::run;
   k.run_plain = &O::run_plain;
   table().push_back(k);
