@@ -27,6 +27,7 @@
 // on the GPU at plan creation; filters of one M come from one batched FFT.
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <new>
@@ -109,6 +110,11 @@ struct gfft_plan_uneven {
   std::vector<Graph> graphs;
   uint64_t tick = 0;
   cudaStream_t cap = nullptr;
+  // Side streams the batch's independent pieces run on, forked from the
+  // caller's stream and joined back to it.
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kSide] = {};
   // Large 7-smooth lengths on the mixed-radix four-step (item mode).
   struct MixLaunch {
     int64_t L;        // column length of the launch
@@ -513,128 +519,191 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
   }
   GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
   GFFT_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+  for (int k = 0; k < gfft_plan_uneven::kSide; ++k) {
+    GFFT_CUDA(cudaStreamCreateWithFlags(&p->side[k], cudaStreamNonBlocking));
+    GFFT_CUDA(cudaEventCreateWithFlags(&p->ev_join[k], cudaEventDisableTiming));
+  }
+  GFFT_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   GFFT_CUDA(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
   return GFFT_OK;
+}
+
+// Pieces of an uneven batch that touch disjoint outputs and buffers; each is
+// a launch sequence on one stream.
+template <typename C, int DIR>
+static gfft_status run_klass(gfft_plan_uneven* p, int k, C* dst, const C* src, cudaStream_t s) {
+  const Klass& K = p->klass[k];
+  k_uneven<C, DIR><<<K.grid, K.cta, K.smem, s>>>(src, dst, K.d_items, int(K.items.size()), p->d_descs,
+                                                 static_cast<const C*>(p->tab), p->counters + k);
+  GFFT_CUDA(cudaGetLastError());
+  return GFFT_OK;
+}
+
+template <typename C, int DIR>
+static gfft_status run_mixc(gfft_plan_uneven* p, C* dst, const C* src, cudaStream_t s) {
+  void* scratch = nullptr;
+  GFFT_CUDA(ws_alloc(&scratch, size_t(p->mix_scratch) * sizeof(C), s));
+  cudaError_t e = cudaSuccess;
+  for (const auto& ml : p->mix_launches) {
+    MixColsParams mp{};
+    mp.src = ml.pass == MIX_PASS1 ? static_cast<const void*>(src) : scratch;
+    mp.dst = ml.pass == MIX_PASS1 ? scratch : static_cast<void*>(dst);
+    mp.tw = static_cast<const C*>(p->tab) + ml.tw;
+    mp.items = p->d_mix_items;
+    mp.blk = ml.d_blk;
+    mp.tab = p->tab;
+    e = exec_mix_cols(p->prec, DIR, ml.pass, ml.L, mp, ml.blocks, s);
+    if (e != cudaSuccess) break;
+  }
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) return cuda_status(e, "k_mix_cols");
+  return GFFT_OK;
+}
+
+template <typename C, int DIR>
+static gfft_status run_bsm(gfft_plan_uneven* p, C* dst, const C* src, cudaStream_t s) {
+  void* buf = nullptr;
+  GFFT_CUDA(ws_alloc(&buf, 2 * size_t(p->bsm_buf) * sizeof(C), s));
+  void* scratch = buf;
+  void* work = static_cast<C*>(buf) + p->bsm_buf;
+  cudaError_t e = cudaSuccess;
+  for (const auto& ch : p->bsm_chunks) {
+    for (const auto& bl : ch.launches) {
+      const C* W = static_cast<const C*>(p->tab) + bl.tw;
+      if (bl.kind == gfft_plan_uneven::kBsInv1) {
+        MixColsParams mp{};
+        mp.src = scratch;
+        mp.dst = work;
+        mp.tw = W;
+        mp.items = p->d_bsm_inv;
+        mp.blk = bl.d_blk;
+        mp.tab = p->tab;
+        e = exec_mix_cols(p->prec, +1, MIX_PASS1, bl.L, mp, bl.blocks, s);
+      } else {
+        MixBsParams bp{};
+        bp.x = src;
+        bp.y = dst;
+        bp.scratch = scratch;
+        bp.work = work;
+        bp.tw = W;
+        bp.inv = DIR > 0;
+        bp.items = p->d_bsm_items;
+        bp.blk = bl.d_blk;
+        bp.tab = p->tab;
+        e = exec_mix_bs(p->prec, bl.kind, bl.L, bp, bl.blocks, s);
+      }
+      if (e != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) break;
+  }
+  cudaFreeAsync(buf, s);
+  if (e != cudaSuccess) return cuda_status(e, "k_mix_bs");
+  return GFFT_OK;
+}
+
+template <typename C, int DIR>
+static gfft_status run_group(gfft_plan_uneven* p, Group& g, C* dst, const C* src, cudaStream_t s) {
+  const int64_t rows = int64_t(g.items.size());
+  C* work = static_cast<C*>(g.work);
+  const C* tab = static_cast<const C*>(p->tab);
+  const bool tp = (g.plan->algo == Algo::TwoPass || g.plan->algo == Algo::L2Pipe) &&
+                  bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1);
+  if (tp) {
+    // on the two-pass FFT: rows read and written in place in the packed
+    // batch, no gather or scatter pass (Bluestein: the chain fused in)
+    void* scratch = nullptr;
+    GFFT_CUDA(ws_alloc(&scratch, bluestein_tp_chunk_bytes(p->prec, g.M, rows), s));
+    BigTwiddle bt;
+    bt.lo = g.plan->bt_lo;
+    bt.hi = g.plan->bt_hi;
+    bt.shift = g.plan->bt_shift;
+    const cudaError_t e =
+        g.bluestein ? exec_bluestein_tp_items(p->prec, g.M, DIR, src, dst, g.d_items, rows, p->tab, g.plan->tw1,
+                                              g.plan->tw2, bt, scratch, work, s)
+                    : exec_twopass_items(p->prec, g.M, DIR, src, dst, g.d_items, rows, g.plan->tw1, g.plan->tw2, bt,
+                                         scratch, s);
+    cudaFreeAsync(scratch, s);
+    GFFT_CUDA(e);
+    return GFFT_OK;
+  }
+  k_big_gather<C, DIR><<<grid1(rows * g.M), 256, 0, s>>>(work, g.M, src, g.d_items, rows, tab, g.bluestein);
+  GFFT_CUDA(cudaGetLastError());
+  if (!g.bluestein) {
+    const gfft_status r = core_exec(g.plan, DIR, work, work, rows, g.M, g.M, s);
+    if (r != GFFT_OK) return r;
+  } else {
+    gfft_status r = core_exec(g.plan, -1, work, work, rows, g.M, g.M, s);
+    if (r != GFFT_OK) return r;
+    k_big_filter<C, DIR><<<grid1(rows * g.M), 256, 0, s>>>(work, g.M, g.d_items, rows, tab);
+    GFFT_CUDA(cudaGetLastError());
+    r = core_exec(g.plan, +1, work, work, rows, g.M, g.M, s);  // includes 1/M
+    if (r != GFFT_OK) return r;
+  }
+  k_big_scatter<C, DIR><<<grid1(rows * g.M), 256, 0, s>>>(dst, work, g.M, g.d_items, rows, tab, g.bluestein);
+  GFFT_CUDA(cudaGetLastError());
+  return GFFT_OK;
+}
+
+using Piece = std::pair<double, std::function<gfft_status(cudaStream_t)>>;
+
+// Runs the pieces on the plan's side streams, forked from `st` and joined
+// back to it (parallel branches when `st` is being captured): longest
+// first, each onto the stream with the least work so far.  Every side
+// stream rejoins `st` even when a piece fails, so a capture stays whole.
+static gfft_status run_pieces(gfft_plan_uneven* p, cudaStream_t st, std::vector<Piece>& pieces) {
+  if (pieces.size() < 2) {
+    for (auto& pc : pieces) {
+      const gfft_status r = pc.second(st);
+      if (r != GFFT_OK) return r;
+    }
+    return GFFT_OK;
+  }
+  std::stable_sort(pieces.begin(), pieces.end(), [](const Piece& a, const Piece& b) { return a.first > b.first; });
+  const int ns = int(std::min<size_t>(pieces.size(), gfft_plan_uneven::kSide));
+  GFFT_CUDA(cudaEventRecord(p->ev_fork, st));
+  for (int k = 0; k < ns; ++k) GFFT_CUDA(cudaStreamWaitEvent(p->side[k], p->ev_fork, 0));
+  std::vector<double> load(ns, 0.0);
+  gfft_status first = GFFT_OK;
+  for (auto& pc : pieces) {
+    const int k = int(std::min_element(load.begin(), load.end()) - load.begin());
+    load[k] += pc.first;
+    if (first == GFFT_OK) first = pc.second(p->side[k]);
+  }
+  for (int k = 0; k < ns; ++k) {
+    const cudaError_t e1 = cudaEventRecord(p->ev_join[k], p->side[k]);
+    const cudaError_t e2 = cudaStreamWaitEvent(st, p->ev_join[k], 0);
+    if (first == GFFT_OK && (e1 != cudaSuccess || e2 != cudaSuccess))
+      first = cuda_status(e1 != cudaSuccess ? e1 : e2, "uneven join");
+  }
+  return first;
 }
 
 template <typename C, int DIR>
 static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStream_t st) {
   GFFT_CUDA(cudaMemsetAsync(p->counters, 0, 2 * sizeof(unsigned), st));
+  // rough costs (elements moved) for spreading the pieces over the streams
+  std::vector<Piece> pieces;
   for (int k = 0; k < 2; ++k) {
     const Klass& K = p->klass[k];
     if (K.items.empty()) continue;
-    k_uneven<C, DIR><<<K.grid, K.cta, K.smem, st>>>(src, dst, K.d_items, int(K.items.size()), p->d_descs,
-                                                    static_cast<const C*>(p->tab), p->counters + k);
-    GFFT_CUDA(cudaGetLastError());
+    double cost = 0;
+    for (const UnevenItem& u : K.items) cost += double(p->descs[u.desc].s.n) * (p->descs[u.desc].bluestein ? 4 : 2);
+    pieces.push_back({cost, [=](cudaStream_t s) { return run_klass<C, DIR>(p, k, dst, src, s); }});
   }
-  if (!p->mix_items.empty()) {
-    void* scratch = nullptr;
-    GFFT_CUDA(ws_alloc(&scratch, size_t(p->mix_scratch) * sizeof(C), st));
-    cudaError_t e = cudaSuccess;
-    for (const auto& ml : p->mix_launches) {
-      MixColsParams mp{};
-      mp.src = ml.pass == MIX_PASS1 ? static_cast<const void*>(src) : scratch;
-      mp.dst = ml.pass == MIX_PASS1 ? scratch : static_cast<void*>(dst);
-      mp.tw = static_cast<const C*>(p->tab) + ml.tw;
-      mp.items = p->d_mix_items;
-      mp.blk = ml.d_blk;
-      mp.tab = p->tab;
-      e = exec_mix_cols(p->prec, DIR, ml.pass, ml.L, mp, ml.blocks, st);
-      if (e != cudaSuccess) break;
-    }
-    cudaFreeAsync(scratch, st);
-    if (e != cudaSuccess) return cuda_status(e, "k_mix_cols");
-  }
+  if (!p->mix_items.empty())
+    pieces.push_back({4.0 * double(p->mix_scratch), [=](cudaStream_t s) { return run_mixc<C, DIR>(p, dst, src, s); }});
   if (!p->bsm_items.empty()) {
-    void* buf = nullptr;
-    GFFT_CUDA(ws_alloc(&buf, 2 * size_t(p->bsm_buf) * sizeof(C), st));
-    void* scratch = buf;
-    void* work = static_cast<C*>(buf) + p->bsm_buf;
-    cudaError_t e = cudaSuccess;
-    for (const auto& ch : p->bsm_chunks) {
-      for (const auto& bl : ch.launches) {
-        const C* W = static_cast<const C*>(p->tab) + bl.tw;
-        if (bl.kind == gfft_plan_uneven::kBsInv1) {
-          MixColsParams mp{};
-          mp.src = scratch;
-          mp.dst = work;
-          mp.tw = W;
-          mp.items = p->d_bsm_inv;
-          mp.blk = bl.d_blk;
-          mp.tab = p->tab;
-          e = exec_mix_cols(p->prec, +1, MIX_PASS1, bl.L, mp, bl.blocks, st);
-        } else {
-          MixBsParams bp{};
-          bp.x = src;
-          bp.y = dst;
-          bp.scratch = scratch;
-          bp.work = work;
-          bp.tw = W;
-          bp.inv = DIR > 0;
-          bp.items = p->d_bsm_items;
-          bp.blk = bl.d_blk;
-          bp.tab = p->tab;
-          e = exec_mix_bs(p->prec, bl.kind, bl.L, bp, bl.blocks, st);
-        }
-        if (e != cudaSuccess) break;
-      }
-      if (e != cudaSuccess) break;
-    }
-    cudaFreeAsync(buf, st);
-    if (e != cudaSuccess) return cuda_status(e, "k_mix_bs");
+    double cost = 0;
+    for (const auto& ch : p->bsm_chunks) cost += 6.0 * double(ch.elems);
+    pieces.push_back({cost, [=](cudaStream_t s) { return run_bsm<C, DIR>(p, dst, src, s); }});
   }
   for (Group& g : p->groups) {
-    const int64_t rows = int64_t(g.items.size());
-    if (rows == 0) continue;
-    C* work = static_cast<C*>(g.work);
-    const C* tab = static_cast<const C*>(p->tab);
-    if (!g.bluestein && (g.plan->algo == Algo::TwoPass || g.plan->algo == Algo::L2Pipe) && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
-      // one large length on the two-pass FFT: rows read and written in
-      // place in the packed batch, no gather or scatter pass
-      void* scratch = nullptr;
-      GFFT_CUDA(ws_alloc(&scratch, bluestein_tp_chunk_bytes(p->prec, g.M, rows), st));
-      BigTwiddle bt;
-      bt.lo = g.plan->bt_lo;
-      bt.hi = g.plan->bt_hi;
-      bt.shift = g.plan->bt_shift;
-      const cudaError_t e = exec_twopass_items(p->prec, g.M, DIR, src, dst, g.d_items, rows, g.plan->tw1,
-                                               g.plan->tw2, bt, scratch, st);
-      cudaFreeAsync(scratch, st);
-      GFFT_CUDA(e);
-      continue;
-    }
-    if (g.bluestein && (g.plan->algo == Algo::TwoPass || g.plan->algo == Algo::L2Pipe) && bluestein_tp_supported(p->prec, g.M, g.plan->tp[0]->n1)) {
-      // the chain fused into the two-pass FFT_M: rows read and written in
-      // place in the packed batch, no gather or scatter pass
-      void* scratch = nullptr;
-      GFFT_CUDA(ws_alloc(&scratch, bluestein_tp_chunk_bytes(p->prec, g.M, rows), st));
-      BigTwiddle bt;
-      bt.lo = g.plan->bt_lo;
-      bt.hi = g.plan->bt_hi;
-      bt.shift = g.plan->bt_shift;
-      const cudaError_t e = exec_bluestein_tp_items(p->prec, g.M, DIR, src, dst, g.d_items, rows, p->tab,
-                                                    g.plan->tw1, g.plan->tw2, bt, scratch, work, st);
-      cudaFreeAsync(scratch, st);
-      GFFT_CUDA(e);
-      continue;
-    }
-    k_big_gather<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(work, g.M, src, g.d_items, rows, tab, g.bluestein);
-    GFFT_CUDA(cudaGetLastError());
-    if (!g.bluestein) {
-      gfft_status s = core_exec(g.plan, DIR, work, work, rows, g.M, g.M, st);
-      if (s != GFFT_OK) return s;
-    } else {
-      gfft_status s = core_exec(g.plan, -1, work, work, rows, g.M, g.M, st);
-      if (s != GFFT_OK) return s;
-      k_big_filter<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(work, g.M, g.d_items, rows, tab);
-      GFFT_CUDA(cudaGetLastError());
-      s = core_exec(g.plan, +1, work, work, rows, g.M, g.M, st);  // includes 1/M
-      if (s != GFFT_OK) return s;
-    }
-    k_big_scatter<C, DIR><<<grid1(rows * g.M), 256, 0, st>>>(dst, work, g.M, g.d_items, rows, tab, g.bluestein);
-    GFFT_CUDA(cudaGetLastError());
+    if (g.items.empty()) continue;
+    Group* gp = &g;
+    pieces.push_back({double(g.items.size()) * double(g.M) * (g.bluestein ? 6 : 4),
+                      [=](cudaStream_t s) { return run_group<C, DIR>(p, *gp, dst, src, s); }});
   }
-  return GFFT_OK;
+  return run_pieces(p, st, pieces);
 }
 
 static gfft_status uneven_dispatch(gfft_plan_uneven* p, int dir, void* dst, const void* src, cudaStream_t st) {
@@ -717,6 +786,11 @@ void gfft_plan_uneven_close(gfft_plan_uneven* p) {
   if (p->tab) cudaFree(p->tab);
   if (p->counters) cudaFree(p->counters);
   if (p->cap) cudaStreamDestroy(p->cap);
+  for (int k = 0; k < gfft_plan_uneven::kSide; ++k) {
+    if (p->side[k]) cudaStreamDestroy(p->side[k]);
+    if (p->ev_join[k]) cudaEventDestroy(p->ev_join[k]);
+  }
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->done) cudaEventDestroy(p->done);
   delete p;
 }
