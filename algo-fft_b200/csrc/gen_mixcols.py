@@ -8,8 +8,10 @@ for the 7-smooth lengths 1025..12288 that are not powers of two (complex128
 up to 6144, the shared memory one transform can have); and
 kernels_mixbs_t0.cu .. kernels_mixbs_t2.cu: the Bluestein chain's passes
 (gfft_mixbs.cuh) for the column lengths its FFT lengths M = M1 x M2 are built
-from (BS_LENGTHS: the multiples of 16 up to 512, whose products come within
-1.5% of the best 7-smooth M on average), with the same schedules.
+from (the 7-smooth multiples of 16 up to 512, whose products come within
+1.5% of the best 7-smooth M on average, less 48, 64 and 96, which never make
+the smallest M >= 2n - 1 for an n beyond the one-CTA Bluestein range), with
+the same schedules.
 
 Schedule rule, from timing the candidates on a B200 (two stages against three
 and four, several tile widths and occupancies, at L = 100..1000):
@@ -173,7 +175,7 @@ def cfg(L, es, extra=0):
 
 
 def bs_lengths():
-    return [L for L in range(48, 513) if smooth7(L) and L % 16 == 0]
+    return [L for L in range(48, 513) if smooth7(L) and L % 16 == 0 and L not in (48, 64, 96)]
 
 
 def main(out=HERE):

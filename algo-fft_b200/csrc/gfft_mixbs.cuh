@@ -4,7 +4,7 @@
 // The reference pads to M = NextPow2(2n - 1) (plan.go:865), which costs
 // 2..4 times n per FFT; any M >= 2n - 1 gives the same product up to
 // rounding.  Here M is the smallest product of two compiled column lengths
-// (multiples of 16 up to 512) that is at least 2n - 1, used when it is below
+// (18 multiples of 16 from 80 to 512) that is at least 2n - 1, used when it is below
 // the power of two: about 0.76 of it on average over primes 8K..131K.  The
 // element-wise steps ride in the passes, as in the power-of-two chain
 // (kernels_bluestein_tp.cu):

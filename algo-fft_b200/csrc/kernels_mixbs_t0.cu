@@ -4,10 +4,8 @@
 namespace gfft {
 
 void mix_bs_part_0(std::vector<MixBsEntry>& v) {
-  v.push_back(mix_bs_entry<MixCfg<MixSched<8, 6>, 16, 8, 0>,
-                            MixCfg<MixSched<8, 6>, 8, 8, 8>>());  // 48
-  v.push_back(mix_bs_entry<MixCfg<MixSched<12, 8>, 16, 7, 0>,
-                            MixCfg<MixSched<12, 8>, 8, 8, 0>>());  // 96
+  v.push_back(mix_bs_entry<MixCfg<MixSched<10, 8>, 16, 7, 0>,
+                            MixCfg<MixSched<10, 8>, 8, 7, 10>>());  // 80
   v.push_back(mix_bs_entry<MixCfg<MixSched<12, 12>, 16, 5, 0>,
                             MixCfg<MixSched<12, 12>, 8, 6, 0>>());  // 144
   v.push_back(mix_bs_entry<MixCfg<MixSched<16, 14>, 16, 3, 16>,

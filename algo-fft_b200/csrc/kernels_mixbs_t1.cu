@@ -4,8 +4,6 @@
 namespace gfft {
 
 void mix_bs_part_1(std::vector<MixBsEntry>& v) {
-  v.push_back(mix_bs_entry<MixCfg<MixSched<8, 8>, 16, 8, 0>,
-                            MixCfg<MixSched<8, 8>, 8, 8, 0>>());  // 64
   v.push_back(mix_bs_entry<MixCfg<MixSched<14, 8>, 16, 7, 0>,
                             MixCfg<MixSched<14, 8>, 8, 8, 0>>());  // 112
   v.push_back(mix_bs_entry<MixCfg<MixSched<16, 10>, 16, 5, 0>,

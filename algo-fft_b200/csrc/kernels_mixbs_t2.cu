@@ -4,8 +4,6 @@
 namespace gfft {
 
 void mix_bs_part_2(std::vector<MixBsEntry>& v) {
-  v.push_back(mix_bs_entry<MixCfg<MixSched<10, 8>, 16, 7, 0>,
-                            MixCfg<MixSched<10, 8>, 8, 7, 10>>());  // 80
   v.push_back(mix_bs_entry<MixCfg<MixSched<16, 8>, 16, 7, 0>,
                             MixCfg<MixSched<16, 8>, 8, 8, 0>>());  // 128
   v.push_back(mix_bs_entry<MixCfg<MixSched<16, 12>, 16, 3, 16>,

@@ -33,7 +33,7 @@ def test_generated_files_are_current(tmp_path):
 def test_bluestein_lengths_are_table_lengths():
     g = _gen()
     bs = g.bs_lengths()
-    assert bs == [L for L in range(48, 513) if g.smooth7(L) and L % 16 == 0] and len(bs) == 21
+    assert bs == [80] + [L for L in range(112, 513) if g.smooth7(L) and L % 16 == 0] and len(bs) == 18
     assert max(bs) ** 2 == 1 << 18  # FFT lengths up to 2^18: n up to 131072
 
 
