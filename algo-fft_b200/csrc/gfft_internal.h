@@ -120,7 +120,7 @@ int mix_cols_width(int prec, int pass, int64_t L);  // columns per tile (0: not 
 cudaError_t exec_mix_cols(int prec, int dir, int pass, int64_t L, MixColsParams p, int64_t count, cudaStream_t st);
 // Bluestein on the compiled tiles (gfft_mixbs.cuh): the smallest FFT length
 // M = M1 x M2 >= 2n - 1 its column lengths build (M1 <= M2 returned in *m1;
-// 0 when none), and one of its passes (BSK_IN / BSK_FILT / BSK_OUT) over
+// 0 when none), and one of its passes (BSK_IN / BSK_MID / BSK_OUT) over
 // `count` transforms, or `count` CTAs in item mode.
 struct MixBsParams;
 // Whole contiguous transforms of a compiled length (rows mode: every

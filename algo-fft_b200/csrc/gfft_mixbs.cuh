@@ -7,25 +7,29 @@
 // (18 multiples of 16 from 80 to 512) that is at least 2n - 1, used when it is below
 // the power of two: about 0.76 of it on average over primes 8K..131K.  The
 // element-wise steps ride in the passes, as in the power-of-two chain
-// (kernels_bluestein_tp.cu):
+// (kernels_bluestein_tp.cu), three launches per chunk of transforms:
 //   BSK_IN   forward pass 1 (columns of M1), its loads the chirp-weighted,
-//            zero-padded input a_m = x_m w_m (m < n), scratch out;
-//   BSK_FILT forward pass 2 (columns of M2), its stores the spectrum times
-//            the filter, Z_k = A_k F_k, in natural order back into the
-//            scratch (a tile writes exactly the addresses it read);
-//   the inverse FFT's pass 1 is the plain column tile (k_mix_cols pass 1,
-//            inverse direction), scratch to work;
-//   BSK_OUT  inverse pass 2, its stores y_k = w_k z_k / M (and 1/n for the
-//            inverse transform) for k < n only.
-// The chirp w and filter F of the forward direction serve the inverse as
-// conj(w) and conj(F[(M - k) mod M]) (flag `inv`).  Index maps are the
-// four-step's: input m = M2 n1 + n2, output k = k1 + M1 k2.
+//            zero-padded input a_m = x_m w_m (m < n), scratch out (rows n2
+//            of M1, times W_M^{n2 k1});
+//   BSK_MID  forward pass 2 on columns k1 of the scratch (length M2), the
+//            spectrum times the filter, Z_k = A_k F_k (k = k1 + M1 k2), left
+//            in shared memory; then the inverse FFT's pass 1 on the same
+//            tile: the inverse splits M the other way (M2 rows of M1), so
+//            its column k1 is exactly the tile's column, times
+//            W_M^{-k1 j2}, stored as rows k1 of M2 into the work buffer;
+//   BSK_OUT  inverse pass 2 (columns of M1), its stores y_k = w_k z_k / M
+//            (and 1/n for the inverse transform) for k < n only, k = j2 +
+//            M2 j1.
+// About 4M + 2n element transfers per transform (6M + 2n with the filter
+// product stored and the inverse pass 1 a launch of its own).  The chirp w
+// and filter F of the forward direction serve the inverse as conj(w) and
+// conj(F[(M - k) mod M]) (flag `inv`).
 #pragma once
 #include "gfft_mixcols.cuh"
 
 namespace gfft {
 
-enum { BSK_IN = 0, BSK_FILT = 1, BSK_OUT = 2 };
+enum { BSK_IN = 0, BSK_MID = 1, BSK_OUT = 2 };
 
 // One transform of an uneven batch on this chain (offsets in elements).
 struct MixBsItem {
@@ -35,7 +39,7 @@ struct MixBsItem {
   int64_t chirp, filt;  // forward chirp (n) and filter spectrum (M) in `tab`
   int64_t lo, hi;       // W_M split tables in `tab`
   int32_t shift;
-  int32_t first[3];     // first CTA in its BSK_IN / BSK_FILT / BSK_OUT launch
+  int32_t first[3];     // first CTA in its BSK_IN / BSK_MID / BSK_OUT launch
 };
 
 struct MixBsParams {
@@ -47,7 +51,7 @@ struct MixBsParams {
   const void* w;      // batch mode: chirp of the direction asked for
   const void* f;      // batch mode: filter spectrum of that direction
   const void* tw;     // W_L, L the launch's column length
-  BigTwiddle bt;      // W_M (BSK_IN)
+  BigTwiddle bt;      // W_M (BSK_IN, BSK_MID)
   int64_t tiles;      // batch mode: column tiles per transform; item mode: CTAs
   double scale;       // batch mode: output scale (1/n for the inverse)
   int inv;            // item mode: 1 for the inverse (conjugate tables, 1/n)
@@ -76,10 +80,12 @@ struct MixBsIn {
   }
 };
 
-template <typename C>
-struct MixBsFilt {
-  static constexpr bool kLoad = false, kStore = true;
-  C* z;
+// BSK_MID's forward stores: Z_k = A_k F_k into the tile's shared memory,
+// row k2 of column c (k = k1 + M1 k2, k1 = col0 + c).
+template <typename TL, typename C>
+struct MixBsFiltSh {
+  static constexpr bool kLoad = false, kStore = true, kShared = true;
+  C* sh;
   const C* f;
   int64_t m1, col0, M;
   int inv;
@@ -88,8 +94,16 @@ struct MixBsFilt {
     // one load per element: the index first, then the conjugate
     C fk = __ldg(f + (inv ? (k == 0 ? 0 : M - k) : k));
     if (inv) fk.y = -fk.y;
-    __stcg(z + k, cmul(v, fk));
+    sh[TL::phys(row, c)] = cmul(v, fk);
   }
+};
+
+// BSK_MID's inverse loads: the same rows back out of shared memory.
+template <typename TL, typename C>
+struct MixBsLoadSh {
+  static constexpr bool kLoad = true, kStore = false, kShared = true;
+  const C* sh;
+  __device__ __forceinline__ C load(int row, int c) const { return sh[TL::phys(row, c)]; }
 };
 
 template <typename C>
@@ -97,11 +111,11 @@ struct MixBsOut {
   static constexpr bool kLoad = false, kStore = true;
   C* y;
   const C* w;
-  int64_t n, m1, col0;
+  int64_t n, m2, col0;
   typename RealOf<C>::type scale;
   int inv;
   __device__ __forceinline__ void store(int row, int c, C v) const {
-    const int64_t k = col0 + c + m1 * int64_t(row);
+    const int64_t k = col0 + c + m2 * int64_t(row);
     if (k < n) st_stream(y + k, cscale(cmul(v, bs_chirp(w, k, inv)), scale));
   }
 };
@@ -144,7 +158,7 @@ __global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_bs(MixBs
     f = static_cast<const C*>(p.f);
     oscale = Re(p.scale);  // batch mode: the direction's own tables
   }
-  const int64_t ncols = M / L;  // M2 for BSK_IN, M1 for the pass-2 kinds
+  const int64_t ncols = M / L;  // M2 for BSK_IN and BSK_OUT, M1 for BSK_MID
   const int c = threadIdx.x % NC, t = threadIdx.x / NC;
   const bool active = col0 + c < ncols;
   const C* tw = static_cast<const C*>(p.tw);
@@ -160,10 +174,20 @@ __global__ void __launch_bounds__(MixTile<SC, NC, TT>::TPB, MINB) k_mix_bs(MixBs
       const int cc = e / L, row = e - cc * L;
       __stcg(yt + e, sh[cc * TL::LP + row]);
     }
-  } else if constexpr (KIND == BSK_FILT) {
-    const MixBsFilt<C> io{scratch + s, f, ncols, col0, M, p.inv};
-    mix_stage<C, SC, TL, -1, 0, MIX_PASS2, MixBsFilt<C>>(v, scratch + s + col0, nullptr, sh, t, c, active, tw,
-                                                         Re(1), bt, 0, ncols, ncols, io);
+  } else if constexpr (KIND == BSK_MID) {
+    const MixBsFiltSh<TL, C> fwd{sh, f, ncols, col0, M, p.inv};
+    mix_stage<C, SC, TL, -1, 0, MIX_PASS2, MixBsFiltSh<TL, C>>(v, scratch + s + col0, nullptr, sh, t, c, active,
+                                                               tw, Re(1), bt, 0, ncols, ncols, fwd);
+    __syncthreads();
+    const MixBsLoadSh<TL, C> back{sh};
+    mix_stage<C, SC, TL, +1, 0, MIX_PASS1, MixBsLoadSh<TL, C>>(v, nullptr, nullptr, sh, t, c, active, tw, Re(1), bt,
+                                                               col0 + c, 0, 0, back);
+    C* yt = static_cast<C*>(p.work) + s + col0 * L;
+    const int nv = int(ncols - col0 < NC ? ncols - col0 : NC);
+    for (int e = threadIdx.x; e < L * nv; e += TL::TPB) {
+      const int cc = e / L, row = e - cc * L;
+      __stcg(yt + e, sh[cc * TL::LP + row]);
+    }
   } else {
     const MixBsOut<C> io{static_cast<C*>(p.y) + off_y, w, n, ncols, col0, oscale, p.inv};
     mix_stage<C, SC, TL, +1, 0, MIX_PASS2, MixBsOut<C>>(v, static_cast<const C*>(p.work) + s + col0, nullptr, sh, t,

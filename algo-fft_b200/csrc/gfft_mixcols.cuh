@@ -28,6 +28,7 @@
 // (internal/fft/mixedradix.go:45-188) inside the four-step of large
 // 7-smooth lengths (internal/kernels/sixstep.go:29-91).
 #pragma once
+#include <type_traits>
 #include "gfft_math.cuh"
 
 namespace gfft {
@@ -89,10 +90,17 @@ enum { MIX_PASS1 = 1, MIX_PASS2 = 2 };
 
 // Hooks of mix_stage: kLoad replaces the first stage's loads by
 // io.load(row, c), kStore the last stage's pass-2 stores by
-// io.store(row, c, value) (the value already scaled for the inverse).
+// io.store(row, c, value) (the value already scaled for the inverse).  A
+// hook that declares kShared = true reads or writes the tile's shared
+// memory, and the stage then adds the barriers that reuse needs.
 struct MixNoIO {
   static constexpr bool kLoad = false, kStore = false;
 };
+
+template <typename IO, typename = void>
+struct io_shared : std::false_type {};
+template <typename IO>
+struct io_shared<IO, std::void_t<decltype(IO::kShared)>> : std::bool_constant<IO::kShared> {};
 
 // One stage of a column tile, then the next (compile-time recursion).
 //   MIX_PASS1: the first stage streams rows `ip` elements apart; the last
@@ -114,6 +122,9 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
   constexpr bool GUARD = NB % T != 0;
   constexpr bool FIRST = S == 0;
   constexpr bool LAST = S == SC::NS - 1;
+  // the stage read shared memory, so it must sync before writing it
+  constexpr bool READ_SH = !FIRST || (io_shared<IO>::value && IO::kLoad);
+  constexpr bool STORE_SH = io_shared<IO>::value && IO::kStore;
 
   // Pass 1's four-step twiddles of the last stage, fetched before its loads
   // so their latency hides behind them: W_N^{n2 (i + r P)} = b * s^r with
@@ -153,6 +164,7 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
   }
 
   if constexpr (LAST && PASS == MIX_PASS2) {
+    if constexpr (STORE_SH && READ_SH) __syncthreads();
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
@@ -168,7 +180,7 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
       }
     }
   } else if constexpr (LAST) {
-    if constexpr (!FIRST) __syncthreads();
+    if constexpr (READ_SH) __syncthreads();
     if (active) {
       // s^r = s^(r mod 8) (s^8)^(r / 8): eight low powers and RS / 8 high
       // ones from product trees, so a large last radix keeps few powers live
@@ -200,7 +212,7 @@ __device__ __forceinline__ void mix_stage(C* v, const C* in, C* out, C* sh, int 
     }
     __syncthreads();
   } else {
-    if constexpr (!FIRST) __syncthreads();
+    if constexpr (READ_SH) __syncthreads();
     if (active) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {

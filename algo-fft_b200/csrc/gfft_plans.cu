@@ -469,8 +469,8 @@ gfft_status init_bluestein(PlanCore* c, int mode) {
 }
 
 // The Bluestein chain on the compiled mixed-radix tiles (gfft_mixbs.cuh):
-// four launches per chunk of transforms, scratch and work of M elements per
-// transform each.
+// three launches per chunk of transforms (column lengths M1, M2, M1),
+// scratch and work of M elements per transform each.
 static gfft_status exec_bluestein_mixed(const PlanCore* c, int dir, void* dst, const void* src, int64_t count,
                                         int64_t idist, int64_t odist, cudaStream_t st) {
   const size_t es = elem_bytes(c->prec);
@@ -506,12 +506,10 @@ static gfft_status exec_bluestein_mixed(const PlanCore* c, int dir, void* dst, c
     e = exec_mix_bs(c->prec, BSK_IN, m1, p, m, st);
     if (e != cudaSuccess) break;
     p.tw = c->tw2;
-    e = exec_mix_bs(c->prec, BSK_FILT, m2, p, m, st);
+    e = exec_mix_bs(c->prec, BSK_MID, m2, p, m, st);
     if (e != cudaSuccess) break;
-    const MixColsParams q{scratch, work, m2, m2, 0, M, M, 0, c->tw1, bt, 1.0};
-    e = exec_mix_cols(c->prec, +1, MIX_PASS1, m1, q, m, st);
-    if (e != cudaSuccess) break;
-    e = exec_mix_bs(c->prec, BSK_OUT, m2, p, m, st);
+    p.tw = c->tw1;
+    e = exec_mix_bs(c->prec, BSK_OUT, m1, p, m, st);
   }
   cudaFreeAsync(buf, st);
   if (e != cudaSuccess) return cuda_status(e, "k_mix_bs");

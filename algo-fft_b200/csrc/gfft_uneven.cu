@@ -128,9 +128,7 @@ struct gfft_plan_uneven {
   std::vector<MixLaunch> mix_launches;  // pass-1 launches first
   int64_t mix_scratch = 0;              // elements of the intermediates
   // Bluestein on mixed FFT lengths (item mode): per chunk of transforms,
-  // launches of the phases BSK_IN, BSK_FILT, the inverse first pass (kind
-  // kBsInv1: k_mix_cols over bsm_inv) and BSK_OUT, in that order.
-  static constexpr int kBsInv1 = 3;
+  // launches of the phases BSK_IN, BSK_MID and BSK_OUT, in that order.
   struct BsmLaunch {
     int kind;
     int64_t L, tw, blocks;
@@ -142,8 +140,6 @@ struct gfft_plan_uneven {
   };
   std::vector<MixBsItem> bsm_items;
   MixBsItem* d_bsm_items = nullptr;
-  std::vector<MixItem> bsm_inv;  // the same transforms' inverse first pass
-  MixItem* d_bsm_inv = nullptr;
   std::vector<BsmChunk> bsm_chunks;
   int64_t bsm_buf = 0;  // elements of the largest chunk
   // Recorded after every call's work: the next call, on whatever stream,
@@ -466,21 +462,9 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
       p->bsm_buf = std::max(p->bsm_buf, sum);
       i = j;
     }
-    p->bsm_inv.resize(p->bsm_items.size());
-    for (size_t i = 0; i < p->bsm_items.size(); ++i) {
-      const MixBsItem& b = p->bsm_items[i];
-      MixItem& m = p->bsm_inv[i];
-      m = MixItem{};
-      m.off = b.s;  // reads the filtered spectrum in the scratch
-      m.y = b.s;    // writes the work buffer
-      m.n = b.M;
-      m.lo = b.lo;
-      m.hi = b.hi;
-      m.shift = b.shift;
-    }
     for (size_t ci = 0; ci < spans.size(); ++ci) {
-      for (int kind : {int(BSK_IN), int(BSK_FILT), gfft_plan_uneven::kBsInv1, int(BSK_OUT)}) {
-        const bool on_m1 = kind == BSK_IN || kind == gfft_plan_uneven::kBsInv1;
+      for (int kind : {int(BSK_IN), int(BSK_MID), int(BSK_OUT)}) {
+        const bool on_m1 = kind != BSK_MID;
         std::map<int64_t, std::vector<size_t>> by_len;
         for (size_t i = spans[ci].first; i < spans[ci].second; ++i) {
           const int64_t m1 = bsm_m1[p->bsm_items[i].n];
@@ -488,14 +472,12 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
         }
         for (auto& kv : by_len) {
           const int64_t L = kv.first;
-          const int nc = kind == gfft_plan_uneven::kBsInv1 ? mix_cols_width(p->prec, MIX_PASS1, L)
-                                                          : mix_bs_width(p->prec, L);
+          const int nc = mix_bs_width(p->prec, L);
           if (nc <= 0) return GFFT_ERR_NOT_IMPLEMENTED;
           std::vector<int32_t> blk;
           for (size_t i : kv.second) {
             const int32_t first = int32_t(blk.size());
-            if (kind == gfft_plan_uneven::kBsInv1) p->bsm_inv[i].first[0] = first;
-            else p->bsm_items[i].first[kind] = first;
+            p->bsm_items[i].first[kind] = first;
             const int64_t tiles = (p->bsm_items[i].M / L + nc - 1) / nc;
             blk.insert(blk.end(), size_t(tiles), int32_t(i));
           }
@@ -512,9 +494,6 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     }
     GFFT_CUDA(cudaMalloc(&p->d_bsm_items, p->bsm_items.size() * sizeof(MixBsItem)));
     GFFT_CUDA(cudaMemcpy(p->d_bsm_items, p->bsm_items.data(), p->bsm_items.size() * sizeof(MixBsItem),
-                         cudaMemcpyHostToDevice));
-    GFFT_CUDA(cudaMalloc(&p->d_bsm_inv, p->bsm_inv.size() * sizeof(MixItem)));
-    GFFT_CUDA(cudaMemcpy(p->d_bsm_inv, p->bsm_inv.data(), p->bsm_inv.size() * sizeof(MixItem),
                          cudaMemcpyHostToDevice));
   }
   GFFT_CUDA(cudaMalloc(&p->counters, 2 * sizeof(unsigned)));
@@ -569,29 +548,17 @@ static gfft_status run_bsm(gfft_plan_uneven* p, C* dst, const C* src, cudaStream
   cudaError_t e = cudaSuccess;
   for (const auto& ch : p->bsm_chunks) {
     for (const auto& bl : ch.launches) {
-      const C* W = static_cast<const C*>(p->tab) + bl.tw;
-      if (bl.kind == gfft_plan_uneven::kBsInv1) {
-        MixColsParams mp{};
-        mp.src = scratch;
-        mp.dst = work;
-        mp.tw = W;
-        mp.items = p->d_bsm_inv;
-        mp.blk = bl.d_blk;
-        mp.tab = p->tab;
-        e = exec_mix_cols(p->prec, +1, MIX_PASS1, bl.L, mp, bl.blocks, s);
-      } else {
-        MixBsParams bp{};
-        bp.x = src;
-        bp.y = dst;
-        bp.scratch = scratch;
-        bp.work = work;
-        bp.tw = W;
-        bp.inv = DIR > 0;
-        bp.items = p->d_bsm_items;
-        bp.blk = bl.d_blk;
-        bp.tab = p->tab;
-        e = exec_mix_bs(p->prec, bl.kind, bl.L, bp, bl.blocks, s);
-      }
+      MixBsParams bp{};
+      bp.x = src;
+      bp.y = dst;
+      bp.scratch = scratch;
+      bp.work = work;
+      bp.tw = static_cast<const C*>(p->tab) + bl.tw;
+      bp.inv = DIR > 0;
+      bp.items = p->d_bsm_items;
+      bp.blk = bl.d_blk;
+      bp.tab = p->tab;
+      e = exec_mix_bs(p->prec, bl.kind, bl.L, bp, bl.blocks, s);
       if (e != cudaSuccess) break;
     }
     if (e != cudaSuccess) break;
@@ -694,7 +661,7 @@ static gfft_status uneven_run(gfft_plan_uneven* p, C* dst, const C* src, cudaStr
     pieces.push_back({4.0 * double(p->mix_scratch), [=](cudaStream_t s) { return run_mixc<C, DIR>(p, dst, src, s); }});
   if (!p->bsm_items.empty()) {
     double cost = 0;
-    for (const auto& ch : p->bsm_chunks) cost += 6.0 * double(ch.elems);
+    for (const auto& ch : p->bsm_chunks) cost += 5.0 * double(ch.elems);
     pieces.push_back({cost, [=](cudaStream_t s) { return run_bsm<C, DIR>(p, dst, src, s); }});
   }
   for (Group& g : p->groups) {
@@ -781,7 +748,6 @@ void gfft_plan_uneven_close(gfft_plan_uneven* p) {
     for (auto& bl : ch.launches)
       if (bl.d_blk) cudaFree(bl.d_blk);
   if (p->d_bsm_items) cudaFree(p->d_bsm_items);
-  if (p->d_bsm_inv) cudaFree(p->d_bsm_inv);
   if (p->d_descs) cudaFree(p->d_descs);
   if (p->tab) cudaFree(p->tab);
   if (p->counters) cudaFree(p->counters);

@@ -73,7 +73,7 @@ using MixBsFn = cudaError_t (*)(const MixBsParams&, int64_t, cudaStream_t);
 struct MixBsEntry {
   int L;
   int nc[2];           // tile width per precision
-  MixBsFn fn[2][3];    // [prec][BSK_IN / BSK_FILT / BSK_OUT]
+  MixBsFn fn[2][3];    // [prec][BSK_IN / BSK_MID / BSK_OUT]
 };
 
 template <typename C, typename CFG, int KIND>
@@ -81,7 +81,7 @@ cudaError_t launch_mix_bs(const MixBsParams& p, int64_t blocks, cudaStream_t st)
   using SC = typename CFG::Sched;
   constexpr int NC = CFG::nc;
   using TL = MixTile<SC, NC, CFG::tt>;
-  constexpr int smem = (KIND == BSK_IN ? TL::ELEMS1 : TL::ELEMS2) * int(sizeof(C));
+  constexpr int smem = (KIND == BSK_OUT ? TL::ELEMS2 : TL::ELEMS1) * int(sizeof(C));
   auto kern = &k_mix_bs<C, SC, NC, KIND, CFG::minb, CFG::tt>;
   static const cudaError_t attr =
       smem > 48 * 1024 ? cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) : cudaSuccess;
@@ -102,10 +102,10 @@ MixBsEntry mix_bs_entry() {
   e.nc[kC64] = F::nc;
   e.nc[kC128] = D::nc;
   e.fn[kC64][BSK_IN] = &launch_mix_bs<float2, F, BSK_IN>;
-  e.fn[kC64][BSK_FILT] = &launch_mix_bs<float2, F, BSK_FILT>;
+  e.fn[kC64][BSK_MID] = &launch_mix_bs<float2, F, BSK_MID>;
   e.fn[kC64][BSK_OUT] = &launch_mix_bs<float2, F, BSK_OUT>;
   e.fn[kC128][BSK_IN] = &launch_mix_bs<double2, D, BSK_IN>;
-  e.fn[kC128][BSK_FILT] = &launch_mix_bs<double2, D, BSK_FILT>;
+  e.fn[kC128][BSK_MID] = &launch_mix_bs<double2, D, BSK_MID>;
   e.fn[kC128][BSK_OUT] = &launch_mix_bs<double2, D, BSK_OUT>;
   return e;
 }

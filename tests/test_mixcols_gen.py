@@ -37,6 +37,51 @@ def test_bluestein_lengths_are_table_lengths():
     assert max(bs) ** 2 == 1 << 18  # FFT lengths up to 2^18: n up to 131072
 
 
+def _primes(n):
+    sieve = np.ones(n + 1, bool)
+    sieve[:2] = False
+    for i in range(2, int(n ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = False
+    return [int(p) for p in np.nonzero(sieve)[0]]
+
+
+def _bs_split(bs, n):
+    """(M, M1) as bs_mixed_length (kernels_mixcols.cu) picks them: the
+    smallest product M1 x M2 >= 2n - 1 of table lengths, M1 <= M2, the most
+    balanced among equal products."""
+    best, a_best = 0, 0
+    for i, a in enumerate(bs):
+        for b in bs[i:]:
+            m = a * b
+            if m >= 2 * n - 1 and (best == 0 or m < best or (m == best and a > a_best)):
+                best, a_best = m, a
+    return best, a_best
+
+
+def test_bluestein_sweep_covers_every_factor_role():
+    """The GPU sweep's primes run every Bluestein factor length in every
+    role (M1: BSK_IN and BSK_OUT, M2: BSK_MID) that some prime beyond the
+    one-CTA range reaches on the mixed chain."""
+    import importlib
+    g = _gen()
+    bs = g.bs_lengths()
+    sweep = importlib.import_module("test_mixcols_sweep_gpu").BS_PRIMES
+    reach, got = set(), set()
+    for n in _primes(131072):
+        if n <= 8192:
+            continue
+        M, a = _bs_split(bs, n)
+        if M and M < 1 << (2 * n - 2).bit_length():
+            roles = {(a, 1), (M // a, 2)}
+            reach |= roles
+            if n in sweep:
+                got |= roles
+    assert got == reach
+    assert {L for L, r in reach if r == 1} == set(bs) - {512}
+    assert {L for L, r in reach if r == 2} == set(bs) - {80, 112, 128}
+
+
 def test_every_length_has_a_launchable_plan():
     g = _gen()
     lengths = [L for L in range(48, 1025) if g.smooth7(L)]

@@ -1,7 +1,9 @@
 """Every compiled mixed-radix kernel against numpy's FP64 FFT: the single
 pass (rows mode) of every 7-smooth length it is built for, both precisions;
 every column length as both passes of the four-step of L x L; and every
-Bluestein factor length through primes whose mixed FFT length uses it.  The
+Bluestein factor length in each role it can take (M1: the chirp-weighted
+first pass and the output pass; M2: the fused middle pass) through primes
+whose mixed FFT length M = M1 x M2 uses it there.  The
 reference runs these lengths through its mixed-radix recursion and
 Bluestein (internal/fft/mixedradix.go:45-188, plan_bluestein.go:7-58)."""
 import numpy as np
@@ -23,8 +25,11 @@ def _smooth7(n):
 TABLE = [L for L in range(48, 1025) if _smooth7(L)]
 ROWS3 = {0: [L for L in range(1025, 12289) if _smooth7(L) and L & (L - 1)],
          1: [L for L in range(1025, 6145) if _smooth7(L) and L & (L - 1)]}
-# primes whose mixed Bluestein length M = M1 x M2 covers every factor length
-BS_PRIMES = [8209, 8963, 9221, 10369, 12289, 15361, 18433, 19207, 20483, 25097, 30727, 48397, 49157, 80021, 80651]
+# primes whose mixed Bluestein lengths M = M1 x M2 (M1 <= M2) take every
+# factor length as M1 and as M2 where some n in 8193..131072 does (512 is
+# never M1, 80, 112 and 128 never M2)
+BS_PRIMES = [8209, 8963, 9221, 10369, 12289, 15361, 17921, 18433, 19207, 20483, 25097, 28687, 30727, 40961, 48397,
+             49157, 72577, 76801, 80021, 80651, 92173, 98317, 114689]
 
 
 def _check(tok, n, prec, count, bound):
