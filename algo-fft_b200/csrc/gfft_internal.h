@@ -133,13 +133,13 @@ int64_t bs_mixed_length(int64_t n, int64_t* m1);
 int mix_bs_width(int prec, int64_t L);
 cudaError_t exec_mix_bs(int prec, int kind, int64_t L, MixBsParams p, int64_t count, cudaStream_t st);
 // Bluestein's FFT length: kBsAuto takes the mixed length (a product of
-// compiled column lengths) when it is at most kBsMixedRatio of
+// compiled column lengths) where bs_mixed_preferred says so against
 // NextPow2(2n - 1), the reference's; kBsPow2 / kBsMixed force either (the
 // latter where a smaller mixed length exists).  bs_mixed_choice: that
 // smaller mixed length (0: none, or the one-CTA fused range).
 enum { kBsAuto = 0, kBsPow2 = 1, kBsMixed = 2 };
-constexpr double kBsMixedRatio = 0.65;
 int64_t bs_mixed_choice(int64_t n, int64_t* m1);
+bool bs_mixed_preferred(int64_t mx, int64_t M);
 gfft_status init_bluestein(PlanCore* c, int mode = kBsAuto);
 // Tensor-core split-fp16 radix-16 form (complex64, powers of two 16 <= n <= 2^24;
 // n = r * 16^s with r = 2, 4, 8 takes one leading FP32 radix-r stage).

@@ -394,17 +394,27 @@ int64_t bs_mixed_choice(int64_t n, int64_t* m1) {
   return M > 16384 && mx > 0 && mx < M ? mx : 0;
 }
 
+// The mixed chain's passes cost more per FFT element than the power-of-two
+// chain's, by a factor that depends on M: the two-pass chain of M = 32768
+// (128 x 256 tiles) runs about 1.3x slower per element than at 2^16..2^18,
+// so there the mixed length wins up to M itself; at 65536 the break-even
+// ratio is near 0.88 (complex64) to above 0.9 (complex128), beyond that
+// 0.70 (measured on 128 MB batches of 30 primes).
+bool bs_mixed_preferred(int64_t mx, int64_t M) {
+  const double r = M <= 32768 ? 1.0 : M <= 65536 ? 0.9 : 0.70;
+  return mx > 0 && double(mx) <= r * double(M);
+}
+
 gfft_status init_bluestein(PlanCore* c, int mode) {
   const int64_t n = c->n;
   int64_t M = 1;
   while (M < 2 * n - 1) M <<= 1;  // plan.go:865 NextPowerOfTwo(2n-1)
   // Beyond the one-CTA fused kernel, a smaller FFT length built from two
-  // compiled column lengths (the product is the same up to rounding).  Its
-  // passes move about 1.35x more time per element than the power-of-two
-  // chain's, so the automatic choice takes it only at <= 0.65 of M.
+  // compiled column lengths (the product is the same up to rounding) where
+  // bs_mixed_preferred expects it to be faster.
   int64_t m1 = 0;
   const int64_t mx = bs_mixed_choice(n, &m1);
-  const bool bsm = mx > 0 && (mode == kBsMixed || (mode == kBsAuto && double(mx) <= kBsMixedRatio * double(M)));
+  const bool bsm = mx > 0 && (mode == kBsMixed || (mode == kBsAuto && bs_mixed_preferred(mx, M)));
   if (bsm) M = mx;
   const size_t es = elem_bytes(c->prec);
   c->sub = new PlanCore;

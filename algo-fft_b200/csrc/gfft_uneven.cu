@@ -235,11 +235,11 @@ static gfft_status uneven_build(gfft_plan_uneven* p) {
     int64_t M = 1;
     while (M < 2 * n - 1) M <<= 1;
     // beyond the one-CTA kernel: a smaller FFT length of two compiled
-    // column lengths where it is at most kBsMixedRatio of M (the plans'
-    // rule; never a power of two itself)
+    // column lengths where the plans' rule prefers it (never a power of
+    // two itself)
     int64_t bm1 = 0;
     const int64_t mx = M > max_direct_bs ? bs_mixed_choice(n, &bm1) : 0;
-    if (mx > 0 && double(mx) <= kBsMixedRatio * double(M)) {
+    if (bs_mixed_preferred(mx, M)) {
       bsm_M[n] = mx;
       bsm_m1[n] = bm1;
       bs_by_m[mx].push_back(n);

@@ -38,9 +38,17 @@ def _mixed_m(n):
     return mx or p2
 
 
+def _preferred(mx, p2):
+    """The automatic choice's rule (bs_mixed_preferred, gfft_plans.cu): the
+    mixed length up to the power of two itself for 32768, 0.9 of it for
+    65536, 0.70 beyond."""
+    r = 1.0 if p2 <= 32768 else 0.9 if p2 <= 65536 else 0.70
+    return mx > 0 and mx <= r * p2
+
+
 def _plan(n, prec=0):
-    """The mixed chain where it exists (forced: the automatic choice takes
-    it only at <= 0.65 of the power of two), else the default plan."""
+    """The mixed chain where it exists (forced: the automatic choice
+    weighs it against the power of two), else the default plan."""
     mx, _ = _lengths(n)
     tok = f"gpu-sm100-bluestein-n{n}-mx" if mx else None
     return algofft.Plan(n, prec, variant=tok)
@@ -57,20 +65,22 @@ def _run(p, x, count, inverse=False):
 
 
 # primes from just past the one-CTA limit (8209: M = 17920 for 32768) to
-# 100003 (200704 for 262144), a composite with a large prime factor, and two
-# lengths whose best product is the power of two itself
-C64 = [8209, 12289, 16411, 20011, 40009, 49233, 100003, 65521, 131071]
+# 100003 (200704 for 262144), a composite with a large prime factor, two
+# lengths whose best product is the power of two itself, and lengths on
+# either side of the rule (28753: 0.88 of 65536, 31657: 0.98, 42043: 0.66
+# of 131072, 45737: 0.70)
+C64 = [8209, 12289, 16411, 20011, 40009, 49233, 100003, 65521, 131071, 28753, 31657, 42043, 45737]
 
 
 @pytest.mark.parametrize("n", C64)
 def test_default_bluestein_length(n):
-    """The automatic choice: the mixed length at <= 0.65 of the power of two
+    """The automatic choice: the mixed length where the rule prefers it
     ("-mx"), else the power of two ("-p2" where a smaller mixed length was
     passed over)."""
     mx, p2 = _lengths(n)
     with algofft.NewPlan(n) as p:
         alg = p.Algorithm()
-    if mx and mx <= 0.65 * p2:
+    if _preferred(mx, p2):
         assert alg.startswith(f"gpu-sm100-bluestein-n{n}-mx-m{mx}+"), alg
     elif mx:
         assert alg.startswith(f"gpu-sm100-bluestein-n{n}-p2-m{p2}+"), alg

@@ -16,12 +16,12 @@ pytestmark = pytest.mark.gpu
 # mixed-radix four-step, one launch per factor length: 13440 = 112 x 120,
 # 21609 = 147 x 147 and 50421 = 147 x 343 share a pass-1 launch, 25000 =
 # 125 x 200 and 40000 = 200 x 200 a pass-2 launch), large primes (Bluestein
-# items on mixed FFT lengths at <= 0.65 of the power of two: 16411 twice at
-# 144 x 240, 20011, 40009; grouped by power-of-two FFT length otherwise:
-# 12289, 65521), repeats of one length
+# items on mixed FFT lengths where the plans' rule prefers them: 16411 twice
+# at 144 x 240, 12289, 20011, 40009; grouped by power-of-two FFT length
+# otherwise: 31657, 65521), repeats of one length
 LENGTHS = [1, 2, 3, 5, 7, 8, 13, 64, 97, 360, 1009, 1024, 2048, 4099, 5003, 6000, 8191, 12289, 16384,
            25000, 32768, 40000, 65521, 65536, 1009, 64, 65536, 360, 131072, 1 << 20, 13440, 21609, 50421,
-           50421, 62500, 40000, 16411, 20011, 40009, 16411]
+           50421, 62500, 40000, 16411, 20011, 40009, 16411, 31657]
 
 
 def _tol(n, c128):
