@@ -98,9 +98,26 @@ def minb(L, sched, nc, es, T, extra=0):
     return k
 
 
-def plan(L, es, extra=0):
-    """(radices, tile width, MINB, threads per column or 0) of one pass;
-    `extra` registers per thread added to the occupancy estimate."""
+# Lengths whose three-stage schedule (schedule3, 8 columns per tile) beat
+# the two-stage one when both forms of the long column lengths were timed,
+# per element size: complex64 480 (24 x 20 on a thread per radix-20
+# butterfly, one CTA per SM) 1.11x in pass 1 and 1.22x in pass 2; for every
+# other length from 240 to 1024 the two-stage form was 4-27% faster.
+# Value: resident CTAs per SM asked of pass 1 and of pass 2.
+THREE = {8: {480: (3, 4)}, 16: {}}
+
+
+def plan(L, es, extra=0, pass_=1):
+    """(radices, tile width, MINB, threads per column or 0) of one column
+    pass (1 or 2); `extra` registers per thread added to the occupancy
+    estimate."""
+    if L in THREE[es]:
+        return schedule3(L), 8, THREE[es][L][pass_ - 1], 0
+    return plan2(L, es, extra)
+
+
+def plan2(L, es, extra=0):
+    """The two-stage plan of plan()."""
     sched = schedule(L)
     nc = (16 if L < 500 else 8) if es == 8 else (8 if L < 500 else 4)
     wide = sched[0] % sched[1] != 0 and L in WIDE[es]
@@ -142,7 +159,7 @@ def rows_plan(L, es):
     shared memory; resident CTAs per SM by the same register estimate, up to
     2048 threads and 200 KB per SM."""
     if L <= 1024:
-        sched, _, _, tt = plan(L, es)
+        sched, _, _, tt = plan2(L, es)
     else:
         sched, tt = schedule3(L), 0
     T = tt if tt else L // max(sched)
@@ -168,8 +185,8 @@ def rows_cfg(L, es):
     return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
 
 
-def cfg(L, es, extra=0):
-    sched, nc, mb, tt = plan(L, es, extra)
+def cfg(L, es, extra=0, pass_=1):
+    sched, nc, mb, tt = plan(L, es, extra, pass_)
     s = ", ".join(str(r) for r in sched)
     return f"MixCfg<MixSched<{s}>, {nc}, {mb}, {tt}>"
 
@@ -182,10 +199,10 @@ def main(out=HERE):
     lengths = [L for L in range(48, 1025) if smooth7(L)]
     parts = [[] for _ in range(PARTS)]
     for i, L in enumerate(lengths):
-        f = cfg(L, 8)
-        d = cfg(L, 16)
-        parts[i % PARTS].append(f"  v.push_back(mix_entry<{f},\n                         {f},\n"
-                                f"                         {d},\n                         {d}>());  // {L}\n")
+        f1, f2 = cfg(L, 8), cfg(L, 8, pass_=2)
+        d1, d2 = cfg(L, 16), cfg(L, 16, pass_=2)
+        parts[i % PARTS].append(f"  v.push_back(mix_entry<{f1},\n                         {f2},\n"
+                                f"                         {d1},\n                         {d2}>());  // {L}\n")
     for k, body in enumerate(parts):
         with open(os.path.join(out, f"kernels_mixcols_t{k}.cu"), "w") as fh:
             fh.write("// Generated by gen_mixcols.py; do not edit.\n"

@@ -14,7 +14,7 @@ void mix_bs_part_1(std::vector<MixBsEntry>& v) {
                             MixCfg<MixSched<20, 16>, 8, 2, 20>>());  // 320
   v.push_back(mix_bs_entry<MixCfg<MixSched<20, 20>, 16, 2, 0>,
                             MixCfg<MixSched<20, 20>, 8, 2, 0>>());  // 400
-  v.push_back(mix_bs_entry<MixCfg<MixSched<24, 20>, 16, 1, 24>,
+  v.push_back(mix_bs_entry<MixCfg<MixSched<10, 8, 6>, 8, 3, 0>,
                             MixCfg<MixSched<24, 20>, 8, 2, 24>>());  // 480
 }
 

@@ -40,8 +40,8 @@ void mix_part_0(std::vector<MixEntry>& v) {
                          MixCfg<MixSched<28, 14>, 16, 3, 0>,
                          MixCfg<MixSched<28, 14>, 8, 2, 0>,
                          MixCfg<MixSched<28, 14>, 8, 2, 0>>());  // 392
-  v.push_back(mix_entry<MixCfg<MixSched<24, 20>, 16, 1, 24>,
-                         MixCfg<MixSched<24, 20>, 16, 1, 24>,
+  v.push_back(mix_entry<MixCfg<MixSched<10, 8, 6>, 8, 3, 0>,
+                         MixCfg<MixSched<10, 8, 6>, 8, 4, 0>,
                          MixCfg<MixSched<24, 20>, 8, 2, 24>,
                          MixCfg<MixSched<24, 20>, 8, 2, 24>>());  // 480
   v.push_back(mix_entry<MixCfg<MixSched<28, 20>, 8, 3, 0>,

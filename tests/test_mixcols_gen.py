@@ -87,9 +87,9 @@ def test_every_length_has_a_launchable_plan():
     lengths = [L for L in range(48, 1025) if g.smooth7(L)]
     assert len(lengths) == 115
     for L in lengths:
-        for es in (8, 16):
-            sched, nc, minb, tt = g.plan(L, es)
-            assert int(np.prod(sched)) == L and len(sched) == 2
+        for es, pass_ in ((8, 1), (8, 2), (16, 1), (16, 2)):
+            sched, nc, minb, tt = g.plan(L, es, pass_=pass_)
+            assert int(np.prod(sched)) == L and len(sched) == (3 if L in g.THREE[es] else 2)
             assert all(g.radix_ok(r) for r in sched)
             T = tt if tt else L // max(sched)
             assert T * nc <= 1024 and 1 <= minb <= 8
