@@ -163,6 +163,13 @@ bool bluestein_fused_supported(int prec, int64_t M);
 // (M = 2^15..2^20, split N1 x M / N1 as the two-pass plans).
 bool bluestein_tp_supported(int prec, int64_t M, int n1);
 size_t bluestein_tp_chunk_bytes(int prec, int64_t M, int64_t count);
+// Bluestein through the plain three-pass FFT_M (M = 2^21..2^24) with the
+// chirp, pad, filter product and output chirp fused into its first and
+// third passes; `sub` is the plain three-pass plan of length M.
+bool bluestein_tp3_supported(int prec, int64_t M);
+gfft_status exec_bluestein_tp3(const PlanCore* sub, const void* src, void* dst, int64_t count, int64_t idist,
+                               int64_t odist, int64_t n, const void* chirp, const void* filt, double scale,
+                               cudaStream_t st);
 cudaError_t exec_bluestein_tp(int prec, int64_t M, const void* src, void* dst, int64_t count, int64_t idist,
                               int64_t odist, int64_t n, const void* chirp, const void* filt, const void* tw1,
                               const void* tw2, BigTwiddle bt, double scale, void* scratch, void* work,

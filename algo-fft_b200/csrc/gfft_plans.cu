@@ -418,7 +418,16 @@ gfft_status init_bluestein(PlanCore* c, int mode) {
   if (bsm) M = mx;
   const size_t es = elem_bytes(c->prec);
   c->sub = new PlanCore;
-  gfft_status s = core_init(c->sub, c->prec, M, c->device);
+  gfft_status s;
+  if (!bsm && bluestein_tp3_supported(c->prec, M)) {
+    // the plain three-pass split, whose first and third passes the chain fuses
+    const ThreePassKernel* k = find_threepass(c->prec, M, -1);
+    s = core_init_variant(c->sub, c->prec, M, c->device,
+                          "gpu-sm100-tp3-" + std::to_string(k->n1) + "x" + std::to_string(k->m1) + "x" +
+                              std::to_string(k->m2));
+  } else {
+    s = core_init(c->sub, c->prec, M, c->device);
+  }
   if (s != GFFT_OK) return s;
   // [chirp fwd | chirp inv | filter fwd | filter inv], then for the mixed
   // chain [W_M1 | W_M2 | W_M low | W_M high]
@@ -557,6 +566,10 @@ static gfft_status exec_bluestein(const PlanCore* c, int dir, void* dst, const v
     if (te != cudaSuccess) return cuda_status(te, "k_bs_tp");
     return GFFT_OK;
   }
+  // three-pass FFT_M: the chain fused into its first and third passes
+  if (c->sub->algo == Algo::ThreePass && !c->sub->t3[0]->tma && bluestein_tp3_supported(c->prec, M))
+    return exec_bluestein_tp3(c->sub, src, dst, count, idist, odist, n, c->bs_w[d], c->bs_f[d],
+                              dir < 0 ? 1.0 : 1.0 / double(n), st);
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t(256) << 20) / (M * int64_t(es))));
   void* work = nullptr;
   GFFT_CUDA(ws_alloc(reinterpret_cast<void**>(&work), size_t(chunk) * size_t(M) * es, st));
