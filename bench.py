@@ -657,7 +657,8 @@ def _convolve(dev, stream, iters, gen):
     return out
 
 
-CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "bs_mixed", "conv_os", "c2r", "r2c", "mlp", "tc4096", "l2p",
+CASES = ("pow2_cols", "uneven600", "uneven20000", "bs_fused", "bs_tp", "bs_mixed", "bs_tp3", "conv_os", "c2r", "r2c", "mlp",
+         "tc4096", "l2p",
          "gen_cols", "mix_cols", "mix_rows", "tp3t", "tp2", "p16384")
 
 
@@ -692,10 +693,11 @@ def run_case(name: str, reps: int) -> int:
         x = cplx(p.Total())
         y = torch.empty_like(x)
         fn = lambda: p.Forward(y, x)  # noqa: E731
-    elif name in ("bs_fused", "bs_tp", "bs_mixed"):
+    elif name in ("bs_fused", "bs_tp", "bs_mixed", "bs_tp3"):
         # Bluestein: n = 8191 (M = 16384, one CTA) / 16411 on M = 65536 (the two-pass power-of-two
-        # chain) / 16411 on M = 34560 = 144 x 240 (the mixed-radix chain)
-        n = 8191 if name == "bs_fused" else 16411
+        # chain) / 16411 on M = 34560 = 144 x 240 (the mixed-radix chain) / 524309 on M = 2^21 (the
+        # three-pass chain, 32 transforms)
+        n = {"bs_fused": 8191, "bs_tp3": 524309}.get(name, 16411)
         count = (1 << 27) // (8 * n)
         x = cplx(n * count)
         y = torch.empty_like(x)
