@@ -105,6 +105,10 @@ def minb(L, sched, nc, es, T, extra=0):
 # other length from 240 to 1024 the two-stage form was 4-27% faster.
 # Value: resident CTAs per SM asked of pass 1 and of pass 2.
 THREE = {8: {480: (3, 4)}, 16: {}}
+# Complex128 lengths whose pass 2 alone ran faster on the three-stage
+# schedule (pass 1 kept the two-stage one at every length): 336 1.16x, 512
+# 1.13x, 1000 1.10x, 768 1.08x.  Value: (tile width, resident CTAs per SM).
+THREE2 = {8: {}, 16: {336: (8, 3), 512: (8, 2), 768: (4, 3), 1000: (4, 2)}}
 
 
 def plan(L, es, extra=0, pass_=1):
@@ -113,6 +117,9 @@ def plan(L, es, extra=0, pass_=1):
     estimate."""
     if L in THREE[es]:
         return schedule3(L), 8, THREE[es][L][pass_ - 1], 0
+    if pass_ == 2 and L in THREE2[es]:
+        nc, mb = THREE2[es][L]
+        return schedule3(L), nc, mb, 0
     return plan2(L, es, extra)
 
 

@@ -63,7 +63,7 @@ void mix_part_0(std::vector<MixEntry>& v) {
   v.push_back(mix_entry<MixCfg<MixSched<40, 25>, 8, 2, 0>,
                          MixCfg<MixSched<40, 25>, 8, 2, 0>,
                          MixCfg<MixSched<40, 25>, 4, 1, 0>,
-                         MixCfg<MixSched<40, 25>, 4, 1, 0>>());  // 1000
+                         MixCfg<MixSched<10, 10, 10>, 4, 2, 0>>());  // 1000
 }
 
 }  // namespace gfft

@@ -35,7 +35,7 @@ void mix_part_1(std::vector<MixEntry>& v) {
   v.push_back(mix_entry<MixCfg<MixSched<21, 16>, 16, 2, 0>,
                          MixCfg<MixSched<21, 16>, 16, 2, 0>,
                          MixCfg<MixSched<21, 16>, 8, 2, 21>,
-                         MixCfg<MixSched<21, 16>, 8, 2, 21>>());  // 336
+                         MixCfg<MixSched<8, 7, 6>, 8, 3, 0>>());  // 336
   v.push_back(mix_entry<MixCfg<MixSched<20, 20>, 16, 2, 0>,
                          MixCfg<MixSched<20, 20>, 16, 2, 0>,
                          MixCfg<MixSched<20, 20>, 8, 2, 0>,

@@ -55,7 +55,7 @@ void mix_part_2(std::vector<MixEntry>& v) {
   v.push_back(mix_entry<MixCfg<MixSched<32, 24>, 8, 2, 0>,
                          MixCfg<MixSched<32, 24>, 8, 2, 0>,
                          MixCfg<MixSched<32, 24>, 4, 2, 32>,
-                         MixCfg<MixSched<32, 24>, 4, 2, 32>>());  // 768
+                         MixCfg<MixSched<12, 8, 8>, 4, 3, 0>>());  // 768
   v.push_back(mix_entry<MixCfg<MixSched<32, 28>, 8, 2, 32>,
                          MixCfg<MixSched<32, 28>, 8, 2, 32>,
                          MixCfg<MixSched<32, 28>, 4, 2, 32>,

@@ -43,7 +43,7 @@ void mix_part_5(std::vector<MixEntry>& v) {
   v.push_back(mix_entry<MixCfg<MixSched<32, 16>, 8, 4, 0>,
                          MixCfg<MixSched<32, 16>, 8, 4, 0>,
                          MixCfg<MixSched<32, 16>, 4, 4, 0>,
-                         MixCfg<MixSched<32, 16>, 4, 4, 0>>());  // 512
+                         MixCfg<MixSched<8, 8, 8>, 8, 2, 0>>());  // 512
   v.push_back(mix_entry<MixCfg<MixSched<25, 25>, 8, 3, 0>,
                          MixCfg<MixSched<25, 25>, 8, 3, 0>,
                          MixCfg<MixSched<25, 25>, 4, 3, 0>,

@@ -89,7 +89,8 @@ def test_every_length_has_a_launchable_plan():
     for L in lengths:
         for es, pass_ in ((8, 1), (8, 2), (16, 1), (16, 2)):
             sched, nc, minb, tt = g.plan(L, es, pass_=pass_)
-            assert int(np.prod(sched)) == L and len(sched) == (3 if L in g.THREE[es] else 2)
+            three = L in g.THREE[es] or (pass_ == 2 and L in g.THREE2[es])
+            assert int(np.prod(sched)) == L and len(sched) == (3 if three else 2)
             assert all(g.radix_ok(r) for r in sched)
             T = tt if tt else L // max(sched)
             assert T * nc <= 1024 and 1 <= minb <= 8
